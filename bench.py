@@ -1,0 +1,414 @@
+"""Benchmark: triangle counting on RMAT scale 24, edge factor 32.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one full triangle count of the degree-oriented RMAT-24 ef32 graph
+(a,b,c,d = .57,.19,.19,.05, seeded, deduplicated, no loops, symmetrised) with
+the graph resident in HBM.  `value` is oriented edges / second over all ranks.
+Multi-GPU (torchrun, one rank per GPU): every rank holds the whole graph and
+counts its shard of the tile plan; the shard counts are summed with one 8-byte
+all-reduce (strong scaling).
+
+`e2e` runs the same count through the public C ABI from pinned HOST buffers:
+symmetric CSR upload (H2D copy, orientation, relabel, padding) + count + the
+8-byte D2H read of the result, every step.
+
+`cpu_baseline` (rank 0, N=1) and `--impl reference` time the reference's own CPU
+implementation (cpuTriCount over the reference's GraphCSR, compiled in place
+under oracle/_ref) on a bounded, evenly strided sample of the same graph's
+vertices, with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "triangle-count edges/sec at RMAT-24: learned-sched vs plain GPU vs CPU; HBM GB/s"
+UNIT = "edges/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--ef", type=int, default=32)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--sched", choices=["plain", "learned"], default="plain")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU sample time")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference GPU kernel")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- plumbing
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, torch):
+        torch.cuda.set_device(self.local)
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def allreduce(self, torch, x: float | int, op: str):
+        if not self.pg:
+            return x
+        dt = torch.float64 if isinstance(x, float) else torch.int64
+        t = torch.tensor([x], dtype=dt, device="cuda")
+        self.pg.all_reduce(t, op={"max": self.pg.ReduceOp.MAX, "sum": self.pg.ReduceOp.SUM}[op])
+        return t.item()
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def build_graph(gb, torch, scale, ef, seed):
+    """RMAT edges generated on the device, symmetric CSR built on the device."""
+    n = 1 << scale
+    src, dst = gb.gen_rmat_device(scale, seed, ef << scale)
+    csr = gb.csr_from_edges_device(src, dst, n)
+    del src, dst
+    torch.cuda.empty_cache()
+    return n, csr
+
+
+def upload_from_device_csr(gb, csr, n):
+    from gary_b200 import _lib
+
+    p, i = csr.device_ptrs()
+    _, nnz = csr.shape()
+    out = C.c_void_p()
+    _lib.check(_lib.load().gary_graph_upload(p, i, n, nnz, _lib.GARY_INPUT_DEVICE, None, C.byref(out)),
+               "gary_graph_upload")
+    return gb.Graph(out.value)
+
+
+def traffic_per_launch(workload: str):
+    f = ROOT / "profiles" / "roofline_traffic.json"
+    if not f.exists():
+        return None
+    try:
+        d = json.loads(f.read_text())
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+def cpu_reference_sample(O, dag_ptr, dag_idx, target_s: float):
+    """Time the reference's cpuTriCount on an evenly strided vertex sample."""
+    import numpy as np
+
+    n = len(dag_ptr) - 1
+    ref = O.RefCSR.from_arrays(dag_ptr.astype(np.int64), dag_idx.astype(np.int32))
+    threads = O.ref_cpu().ref_omp_max_threads()
+    deg = np.diff(dag_ptr.astype(np.int64))
+
+    def run(stride):
+        edges = int(deg[::stride].sum())
+        t0 = time.perf_counter()
+        ref.tri_count(0, n, stride, 0)
+        return edges, time.perf_counter() - t0
+
+    stride = 4096
+    edges, dt = run(stride)
+    while dt < 0.5 and stride > 1:
+        stride = max(1, stride // 8)
+        edges, dt = run(stride)
+    rate = edges / max(dt, 1e-9)
+    total_edges = int(deg.sum())
+    want_edges = rate * target_s
+    stride = max(1, int(total_edges / max(want_edges, 1)))
+    return ref, threads, stride, deg
+
+
+# ---------------------------------------------------------------- arms
+def run_reference(args, dist):
+    """--impl reference: the reference's CPU path, rank 0 only."""
+    import numpy as np
+    import torch
+
+    import gary_b200 as gb
+    from oracle import oracle as O
+
+    if dist.rank != 0:
+        return 0
+    torch.cuda.set_device(dist.local)
+    n, csr = build_graph(gb, torch, args.scale, args.ef, args.seed)
+    g = upload_from_device_csr(gb, csr, n)
+    csr.free()
+    dptr, didx, _ = g.download()
+    m = len(didx)
+    g.free()
+    ref, threads, stride, deg = cpu_reference_sample(O, dptr, didx, args.cpu_seconds / 2)
+    edges = int(deg[::stride].sum())
+    for _ in range(args.warmup):
+        ref.tri_count(0, n, stride * 4, 0)
+    times = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        ref.tri_count(k % stride, n, stride, 0)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times) / len(times)
+    value = edges / dt
+    sample = (f"every {stride}-th vertex of the degree-oriented RMAT-{args.scale} ef{args.ef} DAG "
+              f"(~{edges} of {m} oriented edges per step, offset rotated per step)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"triangle count, RMAT scale {args.scale} edge factor {args.ef}, seed {args.seed}",
+                   "scale": args.scale, "ef": args.ef, "seed": args.seed},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, dist):
+    import numpy as np
+    import torch
+
+    import gary_b200 as gb
+    from gary_b200 import _lib
+
+    dist.init(torch)
+    dev = dist.local
+    sched = {"plain": _lib.GARY_SCHED_PLAIN, "learned": _lib.GARY_SCHED_LEARNED}[args.sched]
+    t_build = time.perf_counter()
+    n, csr = build_graph(gb, torch, args.scale, args.ef, args.seed)
+    _, sym_nnz = csr.shape()
+    g = upload_from_device_csr(gb, csr, n)
+    build_s = time.perf_counter() - t_build
+    info = g.info()
+    m = info["m"]
+    stream = torch.cuda.Stream()
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    L = _lib.load()
+
+    def step():
+        _lib.check(L.gary_count_shard_async(g.handle, _lib.GARY_PATTERN_TRIANGLE, sched, dist.rank,
+                                            dist.world, C.c_void_p(stream.cuda_stream),
+                                            C.c_void_p(out.data_ptr())), "gary_count_shard_async")
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 1)):
+            step()
+    stream.synchronize()
+    count_local = int(out.item())
+
+    # ---- timed region: K steps, device events on the launching stream
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = Clocks(dev)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            evs[k][0].record(stream)
+            step()
+            evs[k][1].record(stream)
+    stream.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    per = [a.elapsed_time(b) for a, b in evs]
+    ms_local = sum(per) / len(per)
+    ms = dist.allreduce(torch, ms_local, "max")
+    count = dist.allreduce(torch, count_local, "sum")
+    value = m / (ms / 1e3)
+
+    # ---- end to end through the public API from pinned host memory
+    e2e = None
+    if args.e2e_steps > 0:
+        hp = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+        hi = torch.empty(sym_nnz, dtype=torch.int32, pin_memory=True)
+        hp_np = hp.numpy().view(np.uint64)
+        hi_np = hi.numpy().view(np.uint32)
+        csr.download(hp_np, hi_np)
+        csr.free()
+        res = C.c_uint64()
+        e2e_times = []
+        for k in range(args.e2e_steps + 1):
+            dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            gh = C.c_void_p()
+            _lib.check(L.gary_graph_upload(hp.data_ptr(), hi.data_ptr(), n, sym_nnz, 0,
+                                           C.c_void_p(stream.cuda_stream), C.byref(gh)), "upload")
+            dres = torch.empty(1, dtype=torch.int64, device="cuda")
+            _lib.check(L.gary_count_shard_async(gh, _lib.GARY_PATTERN_TRIANGLE, sched, dist.rank, dist.world,
+                                                C.c_void_p(stream.cuda_stream), C.c_void_p(dres.data_ptr())),
+                       "count")
+            res.value = int(dres.to("cpu", non_blocking=False).item())  # 8-byte D2H read of the result
+            stream.synchronize()
+            dt = time.perf_counter() - t0
+            L.gary_graph_free(gh)
+            if k > 0:  # first one warms the allocator
+                e2e_times.append(dt)
+            assert res.value == count_local, "e2e count differs from the resident-graph count"
+        e2e_s = dist.allreduce(torch, sum(e2e_times) / len(e2e_times), "max")
+        e2e = {"value": m / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (n + 1) * 8 + sym_nnz * 4,
+               "d2h_bytes_per_step": 8, "ms_per_step": e2e_s * 1e3,
+               "path": "gary_graph_upload(pinned host symmetric CSR) + gary_count_shard_async + D2H of the count"}
+    else:
+        csr.free()
+
+    line = None
+    if dist.rank == 0:
+        workload = f"triangle count, RMAT scale {args.scale} edge factor {args.ef}, seed {args.seed}"
+        alg = info["alg_bytes"]
+        from json import loads
+        peaks = {}
+        pk = ROOT / "MEASURED_PEAKS.json"
+        if pk.exists():
+            peaks = loads(pk.read_text())
+        hbm = peaks.get("hbm_gbs")
+        peak_src = "MEASURED_PEAKS.json hbm_gbs (measured)" if hbm else "fallback 6650 GB/s"
+        hbm = hbm or 6650.0
+        # per-launch kernel time at N ranks: each rank runs one launch over its shard
+        achieved = (alg / dist.world) / (ms_local / 1e3) / 1e9
+        traffic = traffic_per_launch(workload if dist.world == 1 else "")
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "sched": args.sched,
+            "config": {
+                "workload": workload, "scale": args.scale, "ef": args.ef, "seed": args.seed, "n": n,
+                "oriented_edges": m, "sym_nnz": sym_nnz, "max_out_degree": info["max_out_degree"],
+                "wedges": info["wedges"], "alg_bytes": alg,
+                "l2": f"inputs larger than L2: adjacency {info['adj_words'] * 4 / 1e9:.2f} GB vs 0.126 GB L2",
+                "parallelism": f"dp{dist.world} (tile shards, graph replicated)",
+            },
+            "count": count,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
+                         "alg_bytes_per_launch": alg / dist.world},
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": clk,
+            "build_s": build_s,
+        }
+    g_dag = None
+    if dist.rank == 0 and dist.world == 1 and (not args.no_cpu or not args.no_ref_gpu):
+        g_dag = g.download()
+    g.free()
+
+    if dist.rank == 0 and dist.world == 1 and g_dag is not None:
+        from oracle import oracle as O  # CPU baseline / reference leg only
+
+        dptr, didx, _ = g_dag
+        if not args.no_ref_gpu and O.have_ref_gpu():
+            # the reference's own triangleCountHom<true,32> built for sm_100a, same DAG
+            ref = O.RefGpuGraph(dptr.astype(np.int64), didx.astype(np.int32))
+            ref.tri_count(0)
+            tms = []
+            for _ in range(3):
+                c, t = ref.tri_count(0)
+                tms.append(t)
+                assert c == count, f"reference kernel count {c} != ours {count}"
+            ref.free()
+            tr = statistics.median(tms)
+            line["ref_gpu_kernel"] = {"value": m / (tr / 1e3), "unit": UNIT, "ms": tr,
+                                      "kernel": "graph_query::triangleCountHom<true,32> (sm_100a build)",
+                                      "count_equal": True}
+        if not args.no_cpu and O.have_ref_cpu():
+            ref, threads, stride, deg = cpu_reference_sample(O, dptr, didx, args.cpu_seconds)
+            edges = int(deg[::stride].sum())
+            t0 = time.perf_counter()
+            ref.tri_count(0, n, stride, 0)
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {
+                "value": edges / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"every {stride}-th vertex ({edges} oriented edges, {dt:.1f} s) of the same DAG",
+            }
+            ref.free()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    dist.close()
+    return 0
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    if args.impl == "reference":
+        return run_reference(args, dist)
+    return run_ours(args, dist)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,234 @@
+// C-ABI glue: error strings, handle lifetime, dispatch of gary_count.
+// No C++ exception crosses this boundary: every entry point catches and maps
+// to a GARY_ERR_* status (the reference's checkCudaErrors exits the process
+// instead, common/HelperCUDA.h:582-595).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <mutex>
+#include <new>
+
+#include "graph.cuh"
+#include "internal.cuh"
+#include "tc.cuh"
+
+namespace gary {
+
+namespace {
+thread_local char g_error[1024] = {0};
+}
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_error, sizeof(g_error), fmt, ap);
+  va_end(ap);
+}
+
+void clear_error() { g_error[0] = '\0'; }
+
+int device_ordinal() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+
+int sm_count() {
+  static int cache[64] = {0};
+  int d = device_ordinal();
+  if (d >= 0 && d < 64 && cache[d]) return cache[d];
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d) != cudaSuccess || v <= 0) {
+    cudaGetLastError();
+    v = 148;
+  }
+  if (d >= 0 && d < 64) cache[d] = v;
+  return v;
+}
+
+int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
+           cudaStream_t s, gary_graph **out);
+int build_coo(gary_graph *g, cudaStream_t s);
+int download(gary_graph *g, uint64_t *ptr, uint32_t *idx, uint32_t *perm, cudaStream_t s);
+
+void free_plans(gary_graph *g) {
+  for (auto &p : g->plans) {
+    delete p;
+    p = nullptr;
+  }
+}
+
+namespace {
+
+template <typename F>
+int guarded(const char *what, F &&f) {
+  clear_error();
+  try {
+    return f();
+  } catch (const std::bad_alloc &) {
+    set_error("%s: out of memory", what);
+    return GARY_ERR_OOM;
+  } catch (const std::exception &e) {
+    set_error("%s: %s", what, e.what());
+    return GARY_ERR_CUDA;
+  } catch (...) {
+    set_error("%s: unknown exception", what);
+    return GARY_ERR_CUDA;
+  }
+}
+
+int plan_slot(int pattern, int sched) { return (pattern - 3) * 2 + sched; }
+
+int count_async(gary_graph *g, int pattern, int sched, cudaStream_t s, unsigned long long *d_out,
+                uint32_t shard = 0, uint32_t nshards = 1) {
+  GARY_CHECK_ARG(g != nullptr, "graph is NULL");
+  GARY_CHECK_ARG(d_out != nullptr, "output pointer is NULL");
+  GARY_CHECK_ARG(pattern == GARY_PATTERN_TRIANGLE || pattern == GARY_PATTERN_4CYCLE ||
+                     pattern == GARY_PATTERN_4CLIQUE,
+                 "unknown pattern %d", pattern);
+  GARY_CHECK_ARG(sched == GARY_SCHED_PLAIN || sched == GARY_SCHED_LEARNED, "unknown scheduler %d",
+                 sched);
+  GARY_CHECK_ARG(nshards >= 1 && shard < nshards, "shard %u of %u is out of range", shard, nshards);
+  if (pattern != GARY_PATTERN_TRIANGLE || sched != GARY_SCHED_PLAIN) {
+    set_error("pattern %d with scheduler %d is not available in this build", pattern, sched);
+    return GARY_ERR_UNSUPPORTED;
+  }
+  const int slot = plan_slot(pattern, sched);
+  if (!g->plans[slot]) GARY_TRY(build_plain_plan(g, PlanParams{}, s, &g->plans[slot]));
+  return launch_plain_k3(g, g->plans[slot], d_out, s, shard, nshards);
+}
+
+}  // namespace
+}  // namespace gary
+
+using gary::guarded;
+
+extern "C" const char *gary_last_error(void) { return gary::g_error; }
+
+extern "C" int gary_abi_version(void) { return GARY_ABI_VERSION; }
+
+extern "C" int gary_graph_upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n,
+                                 uint64_t nnz, uint32_t flags, void *stream, gary_graph **out) {
+  return guarded("gary_graph_upload", [&] {
+    return gary::upload(ptr, idx, n, nnz, flags, gary::as_stream(stream), out);
+  });
+}
+
+extern "C" int gary_graph_free(gary_graph *g) {
+  if (!g) return GARY_OK;
+  return guarded("gary_graph_free", [&] {
+    gary::free_plans(g);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    delete g;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      gary::set_error("gary_graph_free: %s", cudaGetErrorString(e));
+      return GARY_ERR_CUDA;
+    }
+    return GARY_OK;
+  });
+}
+
+extern "C" int gary_graph_get_info(const gary_graph *g, gary_graph_info *out) {
+  GARY_CHECK_ARG(g != nullptr && out != nullptr, "NULL argument");
+  out->n = g->n;
+  out->max_degree = g->max_degree;
+  out->max_out_degree = g->max_out;
+  out->relabeled = g->relabeled ? 1u : 0u;
+  out->m = g->m;
+  out->adj_words = g->adj_words;
+  out->wedges = g->wedges;
+  out->out_deg_sq = g->out_deg_sq;
+  out->alg_bytes = g->alg_bytes;
+  out->device_bytes = g->device_bytes();
+  return GARY_OK;
+}
+
+extern "C" int gary_graph_device_csr(gary_graph *g, gary_device_csr *out) {
+  GARY_CHECK_ARG(g != nullptr && out != nullptr, "NULL argument");
+  out->m = g->n;
+  out->nnz = g->m;
+  out->indPtr = g->indptr.p;
+  out->colIdx = g->adj.p;
+  out->deg = g->outdeg.p;
+  return GARY_OK;
+}
+
+extern "C" int gary_graph_device_coo(gary_graph *g, gary_device_coo *out) {
+  GARY_CHECK_ARG(g != nullptr && out != nullptr, "NULL argument");
+  return guarded("gary_graph_device_coo", [&] {
+    GARY_TRY(gary::build_coo(g, nullptr));
+    out->m = g->n;
+    out->nnz = g->m;
+    out->rowIdx = g->coo_row.p;
+    out->colIdx = g->coo_col.p;
+    out->deg = g->outdeg.p;
+    return GARY_OK;
+  });
+}
+
+extern "C" int gary_graph_download(gary_graph *g, uint64_t *ptr, uint32_t *idx, uint32_t *perm) {
+  GARY_CHECK_ARG(g != nullptr, "graph is NULL");
+  return guarded("gary_graph_download", [&] { return gary::download(g, ptr, idx, perm, nullptr); });
+}
+
+extern "C" int gary_count_async(gary_graph *g, int pattern, int sched, void *stream,
+                                uint64_t *d_out) {
+  return guarded("gary_count_async", [&] {
+    return gary::count_async(g, pattern, sched, gary::as_stream(stream),
+                             reinterpret_cast<unsigned long long *>(d_out));
+  });
+}
+
+extern "C" int gary_count(gary_graph *g, int pattern, int sched, void *stream, uint64_t *out) {
+  GARY_CHECK_ARG(out != nullptr, "out is NULL");
+  GARY_CHECK_ARG(g != nullptr, "graph is NULL");
+  return guarded("gary_count", [&] {
+    cudaStream_t s = gary::as_stream(stream);
+    if (!g->result.p) GARY_TRY(g->result.alloc_persistent(1));
+    GARY_TRY(gary::count_async(g, pattern, sched, s, g->result.p));
+    unsigned long long h = 0;
+    gary::SchedState st{};
+    gary_count_plan *plan = g->plans[gary::plan_slot(pattern, sched)];
+    GARY_CUDA(cudaMemcpyAsync(&h, g->result.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaMemcpyAsync(&st, plan->sched.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaStreamSynchronize(s));
+    if (st.error) {
+      gary::set_error("a bounded device wait expired (error word 0x%x)", st.error);
+      return GARY_ERR_TIMEOUT;
+    }
+    *out = h;
+    return GARY_OK;
+  });
+}
+
+extern "C" int gary_count_shard_async(gary_graph *g, int pattern, int sched, uint32_t shard,
+                                      uint32_t nshards, void *stream, uint64_t *d_out) {
+  return guarded("gary_count_shard_async", [&] {
+    return gary::count_async(g, pattern, sched, gary::as_stream(stream),
+                             reinterpret_cast<unsigned long long *>(d_out), shard, nshards);
+  });
+}
+
+extern "C" int gary_count_last_stats(gary_graph *g, gary_count_stats *out) {
+  GARY_CHECK_ARG(g != nullptr && out != nullptr, "NULL argument");
+  if (g->last_timed) {
+    float ms = 0.f;
+    cudaError_t e = cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    if (e == cudaErrorNotReady) {
+      cudaGetLastError();
+      gary::set_error("the last counting kernel has not finished; synchronise its stream first");
+      return GARY_ERR_INVALID;
+    }
+    if (e != cudaSuccess) {
+      gary::set_error("cudaEventElapsedTime: %s", cudaGetErrorString(e));
+      cudaGetLastError();
+      return GARY_ERR_CUDA;
+    }
+    g->last.kernel_ms = ms;
+  }
+  *out = g->last;
+  return GARY_OK;
+}

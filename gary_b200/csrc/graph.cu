@@ -1,0 +1,657 @@
+// Graph construction on the device: symmetric CSR from an edge list, and the
+// degree-oriented, relabeled, padded upload.  Replaces the reference's host
+// pipeline (src/Graph.cpp:19-91 symmetrize / orientation / toCSR_, and
+// src/DeviceGraph.cu:18-47 loadFromHost / populateDevice) with sort-based
+// device passes: every step is a coalesced sweep or a CUB radix sort.
+#include <cub/cub.cuh>
+#include <thrust/execution_policy.h>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/reverse_iterator.h>
+#include <thrust/reduce.h>
+#include <thrust/remove.h>
+#include <thrust/scan.h>
+#include <thrust/sequence.h>
+#include <thrust/transform_reduce.h>
+#include <thrust/unique.h>
+
+#include <algorithm>
+#include <exception>
+#include <new>
+
+#include "graph.cuh"
+
+struct gary_csr {
+  int device = 0;
+  uint32_t n = 0;
+  uint64_t nnz = 0;
+  gary::DevBuf<uint64_t> ptr;
+  gary::DevBuf<uint32_t> idx;
+};
+
+namespace gary {
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned grid_for(uint64_t items, int threads = kThreads) {
+  uint64_t b = (items + threads - 1) / threads;
+  uint64_t cap = (uint64_t)sm_count() * 16;
+  if (b > cap) b = cap;
+  return (unsigned)std::max<uint64_t>(b, 1);
+}
+
+inline int bits_for(uint64_t x) {  // bits needed to hold values in [0, x)
+  int b = 0;
+  while (b < 64 && (x - 1) >> b) ++b;
+  return std::max(b, 1);
+}
+
+struct MaxU32 {
+  __host__ __device__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
+};
+struct MinU64 {
+  __host__ __device__ uint64_t operator()(uint64_t a, uint64_t b) const { return a < b ? a : b; }
+};
+
+// error bits written by validation kernels
+enum : unsigned {
+  kErrRange = 1u,
+  kErrLoop = 2u,
+  kErrOrder = 4u,
+  kErrPtr = 8u,
+  kErrDup = 16u,
+  kErrAsym = 32u,
+};
+
+__global__ void k_degree(const uint64_t *__restrict__ ptr, uint32_t n, uint64_t nnz,
+                         uint32_t *__restrict__ deg, unsigned *err) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t a = ptr[v], b = ptr[v + 1];
+    if (b < a || b > nnz) {
+      atomicOr(err, kErrPtr);
+      deg[v] = 0;
+    } else {
+      deg[v] = (uint32_t)(b - a);
+    }
+  }
+}
+
+__global__ void k_indegree(const uint32_t *__restrict__ idx, uint64_t nnz, uint32_t n,
+                           uint32_t *__restrict__ deg, unsigned *err) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < nnz;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t b = idx[e];
+    if (b < n)
+      atomicAdd(&deg[b], 1u);
+    else
+      atomicOr(err, kErrRange);
+  }
+}
+
+__global__ void k_row_heads(const uint64_t *__restrict__ ptr, uint32_t n,
+                            uint32_t *__restrict__ rowid) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t a = ptr[v];
+    if (ptr[v + 1] > a) rowid[a] = (uint32_t)v;
+  }
+}
+
+__global__ void k_rank_scatter(const uint32_t *__restrict__ perm, uint32_t n,
+                               uint32_t *__restrict__ rank) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    rank[perm[i]] = (uint32_t)i;
+}
+
+__device__ __forceinline__ bool before(uint32_t a, uint32_t b, const uint32_t *deg) {
+  uint32_t da = deg[a], db = deg[b];
+  return da < db || (da == db && a < b);
+}
+
+// One key per CSR entry: kept entries (a before b) become (rank a, rank b),
+// the others ~0.  Symmetric input keeps exactly one copy of every edge.
+// `dag` input keeps every entry, oriented.
+__global__ void k_make_keys(const uint32_t *__restrict__ rowid, const uint32_t *__restrict__ idx,
+                            uint64_t nnz, uint32_t n, const uint32_t *__restrict__ deg,
+                            const uint32_t *__restrict__ rank, int lg, bool dag, bool validate,
+                            uint64_t *__restrict__ keys, unsigned *err) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < nnz;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = rowid[e], b = idx[e];
+    if (b >= n) {
+      atomicOr(err, kErrRange);
+      keys[e] = ~0ull;
+      continue;
+    }
+    if (a == b) {
+      atomicOr(err, kErrLoop);
+      keys[e] = ~0ull;
+      continue;
+    }
+    if (validate && e + 1 < nnz && rowid[e + 1] == a && idx[e + 1] <= b) atomicOr(err, kErrOrder);
+    bool fwd = before(a, b, deg);
+    if (!fwd && !dag) {
+      keys[e] = ~0ull;
+      continue;
+    }
+    uint32_t s = fwd ? a : b, t = fwd ? b : a;
+    if (rank) {
+      s = rank[s];
+      t = rank[t];
+    }
+    keys[e] = ((uint64_t)s << lg) | t;
+  }
+}
+
+__global__ void k_check_unique(const uint64_t *__restrict__ keys, uint64_t m, unsigned *err) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i + 1 < m;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    if (keys[i] == keys[i + 1]) atomicOr(err, kErrDup);
+}
+
+// rowstart[u] = index of the first key of row u (or of the next row); keys sorted.
+__global__ void k_key_heads(const uint64_t *__restrict__ keys, uint64_t m, int lg,
+                            uint64_t *__restrict__ rowstart) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t u = keys[i] >> lg;
+    if (i == 0 || (keys[i - 1] >> lg) != u) rowstart[u] = i;
+  }
+}
+
+__global__ void k_rows(const uint64_t *__restrict__ rowstart, uint32_t n,
+                       uint32_t *__restrict__ dplus, uint64_t *__restrict__ plen4) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t d = (uint32_t)(rowstart[u + 1] - rowstart[u]);
+    dplus[u] = d;
+    plen4[u] = (d + 3u) >> 2;
+  }
+}
+
+__global__ void k_scatter_adj(const uint64_t *__restrict__ keys, uint64_t m, int lg,
+                              const uint64_t *__restrict__ rowstart,
+                              const uint64_t *__restrict__ off4, uint32_t *__restrict__ adj) {
+  const uint64_t mask = (1ull << lg) - 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t k = keys[i];
+    uint64_t u = k >> lg;
+    adj[off4[u] * 4 + (i - rowstart[u])] = (uint32_t)(k & mask);
+  }
+}
+
+__global__ void k_row_records(const uint64_t *__restrict__ off4, const uint32_t *__restrict__ dplus,
+                              uint32_t n, uint2 *__restrict__ row, uint64_t *__restrict__ indptr) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u <= n;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    indptr[u] = off4[u] * 4;
+    if (u < n) row[u] = make_uint2((uint32_t)off4[u], dplus[u]);
+  }
+}
+
+// wedge[u] = sum of d+(v) over v in N+(u).  Keys are sorted, so equal rows
+// are contiguous lanes: a segmented warp scan leaves each run's sum in its
+// last lane, which issues one atomic per run.
+__global__ void k_wedges(const uint64_t *__restrict__ keys, uint64_t m, int lg,
+                         const uint32_t *__restrict__ dplus, unsigned long long *__restrict__ wedge) {
+  const uint64_t mask = (1ull << lg) - 1;
+  const int lane = threadIdx.x & 31;
+  uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < m; base += stride) {
+    uint64_t i = base + threadIdx.x;
+    bool ok = i < m;
+    uint64_t k = ok ? keys[i] : ~0ull;
+    uint32_t u = ok ? (uint32_t)(k >> lg) : 0xFFFFFFFFu;
+    unsigned long long v = ok ? dplus[k & mask] : 0ull;
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned long long t = __shfl_up_sync(kFull, v, o);
+      uint32_t tu = __shfl_up_sync(kFull, u, o);
+      if (lane >= o && tu == u) v += t;
+    }
+    uint32_t nu = __shfl_down_sync(kFull, u, 1);
+    bool tail = lane == 31 || nu != u;
+    if (ok && tail && v) atomicAdd(&wedge[u], v);
+  }
+}
+
+struct Sq {
+  __host__ __device__ uint64_t operator()(uint32_t d) const { return (uint64_t)d * d; }
+};
+
+// ---- CUB helpers with stream-ordered temporaries ------------------------
+int radix_sort_keys(DevBuf<uint64_t> &keys, DevBuf<uint64_t> &alt, uint64_t m, int end_bit,
+                    cudaStream_t s) {
+  cub::DoubleBuffer<uint64_t> db(keys.p, alt.p);
+  size_t tmp = 0;
+  GARY_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, db, m, 0, end_bit, s));
+  DevBuf<uint8_t> t;
+  GARY_TRY(t.alloc(tmp, s));
+  GARY_CUDA(cub::DeviceRadixSort::SortKeys(t.p, tmp, db, m, 0, end_bit, s));
+  if (db.Current() != keys.p) std::swap(keys, alt);
+  return GARY_OK;
+}
+
+int row_starts(const DevBuf<uint64_t> &keys, uint64_t m, uint32_t n, int lg,
+               DevBuf<uint64_t> &rowstart, cudaStream_t s, bool persistent = false) {
+  if (persistent) GARY_TRY(rowstart.alloc_persistent((uint64_t)n + 1));
+  else GARY_TRY(rowstart.alloc((uint64_t)n + 1, s));
+  // fill with m, heads, then reverse min-scan so empty rows point at the next row
+  thrust::fill(thrust::cuda::par_nosync.on(s), rowstart.p, rowstart.p + n + 1, m);
+  if (m) k_key_heads<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, rowstart.p);
+  auto rb = thrust::make_reverse_iterator(rowstart.p + n + 1);
+  thrust::inclusive_scan(thrust::cuda::par_nosync.on(s), rb, rb + n + 1, rb, MinU64());
+  GARY_CUDA(cudaGetLastError());
+  return GARY_OK;
+}
+
+int read_err(unsigned *d_err, cudaStream_t s, unsigned *h) {
+  GARY_CUDA(cudaMemcpyAsync(h, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  return GARY_OK;
+}
+
+int input_error(unsigned bits) {
+  set_error("malformed graph input:%s%s%s%s%s%s", (bits & kErrRange) ? " id>=n" : "",
+            (bits & kErrLoop) ? " self-loop" : "", (bits & kErrOrder) ? " unsorted-list" : "",
+            (bits & kErrPtr) ? " bad-ptr" : "", (bits & kErrDup) ? " duplicate-edge" : "",
+            (bits & kErrAsym) ? " not-symmetric" : "");
+  return GARY_ERR_INPUT;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Oriented upload.  Input CSR (symmetric or DAG) -> degree-oriented padded lists.
+int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
+           cudaStream_t s, gary_graph **out) {
+  const bool on_dev = flags & GARY_INPUT_DEVICE;
+  const bool dag = flags & GARY_INPUT_DAG;
+  const bool relabel = !(flags & GARY_KEEP_IDS);
+  const bool validate = flags & GARY_VALIDATE;
+  GARY_CHECK_ARG(out != nullptr, "out is NULL");
+  GARY_CHECK_ARG(n > 0 && n < 0xFFFFFFFFu, "n must be in [1, 2^32-1)");
+  GARY_CHECK_ARG(ptr != nullptr, "ptr is NULL");
+  GARY_CHECK_ARG(nnz == 0 || idx != nullptr, "idx is NULL");
+  if (!on_dev) {
+    GARY_CHECK_ARG(ptr[0] == 0 && ptr[n] == nnz, "ptr[0] must be 0 and ptr[n] must equal nnz");
+  }
+  *out = nullptr;
+
+  auto g = std::make_unique<gary_graph>();
+  GARY_CUDA(cudaGetDevice(&g->device));
+  g->n = n;
+  g->flags = flags;
+  g->relabeled = relabel;
+  auto pol = thrust::cuda::par_nosync.on(s);
+
+  // 1. input on the device
+  DevBuf<uint64_t> dptr_own;
+  DevBuf<uint32_t> didx_own;
+  const uint64_t *dptr = ptr;
+  const uint32_t *didx = idx;
+  if (!on_dev) {
+    GARY_TRY(dptr_own.alloc((uint64_t)n + 1, s));
+    GARY_TRY(didx_own.alloc(nnz, s));
+    GARY_CUDA(cudaMemcpyAsync(dptr_own.p, ptr, ((uint64_t)n + 1) * 8, cudaMemcpyHostToDevice, s));
+    if (nnz)
+      GARY_CUDA(cudaMemcpyAsync(didx_own.p, idx, nnz * 4, cudaMemcpyHostToDevice, s));
+    dptr = dptr_own.p;
+    didx = didx_own.p;
+  }
+
+  DevBuf<unsigned> err;
+  GARY_TRY(err.alloc(1, s));
+  GARY_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), s));
+
+  // 2. degrees (undirected)
+  DevBuf<uint32_t> deg;
+  GARY_TRY(deg.alloc(n, s));
+  k_degree<<<grid_for(n), kThreads, 0, s>>>(dptr, n, nnz, deg.p, err.p);
+  if (dag && nnz) k_indegree<<<grid_for(nnz), kThreads, 0, s>>>(didx, nnz, n, deg.p, err.p);
+  GARY_CUDA(cudaGetLastError());
+  if (on_dev) {
+    uint64_t ends[2];
+    GARY_CUDA(cudaMemcpyAsync(&ends[0], dptr, 8, cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaMemcpyAsync(&ends[1], dptr + n, 8, cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaStreamSynchronize(s));
+    GARY_CHECK_ARG(ends[0] == 0 && ends[1] == nnz, "ptr[0] must be 0 and ptr[n] must equal nnz");
+  }
+  g->max_degree = thrust::reduce(pol, deg.p, deg.p + n, 0u, MaxU32());
+
+  // 3. relabel: rank by (degree, id) with a stable radix sort on degree
+  DevBuf<uint32_t> rank;
+  if (relabel) {
+    DevBuf<uint32_t> dk, dk2, perm2;
+    GARY_TRY(dk.alloc(n, s));
+    GARY_TRY(dk2.alloc(n, s));
+    GARY_TRY(g->perm.alloc_persistent(n));
+    GARY_TRY(perm2.alloc_persistent(n));
+    GARY_CUDA(cudaMemcpyAsync(dk.p, deg.p, (uint64_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    thrust::sequence(pol, perm2.p, perm2.p + n, 0u);
+    cub::DoubleBuffer<uint32_t> kb(dk.p, dk2.p), vb(perm2.p, g->perm.p);
+    size_t tmp = 0;
+    int eb = bits_for((uint64_t)g->max_degree + 1);
+    GARY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kb, vb, n, 0, eb, s));
+    DevBuf<uint8_t> t;
+    GARY_TRY(t.alloc(tmp, s));
+    GARY_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kb, vb, n, 0, eb, s));
+    if (vb.Current() != g->perm.p) std::swap(g->perm, perm2);
+    GARY_TRY(rank.alloc(n, s));
+    k_rank_scatter<<<grid_for(n), kThreads, 0, s>>>(g->perm.p, n, rank.p);
+    GARY_CUDA(cudaGetLastError());
+  }
+
+  // 4. row id of every entry: heads, then an inclusive max-scan
+  const int lg = bits_for(n);
+  DevBuf<uint64_t> keys;
+  uint64_t m = 0;
+  {
+    DevBuf<uint32_t> rowid;
+    GARY_TRY(rowid.alloc(nnz, s));
+    if (nnz) {
+      GARY_CUDA(cudaMemsetAsync(rowid.p, 0, nnz * 4, s));
+      k_row_heads<<<grid_for(n), kThreads, 0, s>>>(dptr, n, rowid.p);
+      size_t tmp = 0;
+      GARY_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
+      DevBuf<uint8_t> t;
+      GARY_TRY(t.alloc(tmp, s));
+      GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
+    }
+    // 5. oriented keys, compacted
+    GARY_TRY(keys.alloc(std::max<uint64_t>(nnz, 1), s));
+    if (nnz) {
+      k_make_keys<<<grid_for(nnz), kThreads, 0, s>>>(rowid.p, didx, nnz, n, deg.p,
+                                                     relabel ? rank.p : nullptr, lg, dag, validate,
+                                                     keys.p, err.p);
+      GARY_CUDA(cudaGetLastError());
+      m = thrust::remove(pol, keys.p, keys.p + nnz, ~0ull) - keys.p;
+    }
+  }
+  dptr_own.release();
+  didx_own.release();
+  unsigned herr = 0;
+  GARY_TRY(read_err(err.p, s, &herr));
+  if (herr) return input_error(herr);
+  if (!dag && 2 * m != nnz) return input_error(kErrAsym);
+
+  // 6. sort (row, col) keys; validate uniqueness
+  {
+    DevBuf<uint64_t> alt;
+    GARY_TRY(alt.alloc(std::max<uint64_t>(m, 1), s));
+    if (m) GARY_TRY(radix_sort_keys(keys, alt, m, 2 * lg, s));
+  }
+  if (validate || dag) {
+    if (m > 1) k_check_unique<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, err.p);
+    GARY_TRY(read_err(err.p, s, &herr));
+    if (herr) return input_error(herr);
+  }
+  g->m = m;
+
+  // 7. rows, padded offsets, adjacency
+  DevBuf<uint64_t> rowstart, off4;
+  DevBuf<uint32_t> dplus;
+  GARY_TRY(row_starts(keys, m, n, lg, rowstart, s));
+  GARY_TRY(dplus.alloc_persistent(n));
+  GARY_TRY(off4.alloc((uint64_t)n + 1, s));
+  k_rows<<<grid_for(n), kThreads, 0, s>>>(rowstart.p, n, dplus.p, off4.p);
+  thrust::exclusive_scan(pol, off4.p, off4.p + n + 1, off4.p, 0ull);
+  uint64_t quads = 0;
+  GARY_CUDA(cudaMemcpyAsync(&quads, off4.p + n, 8, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  if (quads >= (1ull << 32)) {
+    set_error("graph too large: %llu padded words", (unsigned long long)quads * 4);
+    return GARY_ERR_UNSUPPORTED;
+  }
+  g->adj_words = quads * 4;
+  GARY_TRY(g->adj.alloc_persistent(std::max<uint64_t>(g->adj_words, 4)));
+  GARY_CUDA(cudaMemsetAsync(g->adj.p, 0xFF, g->adj.bytes(), s));
+  if (m) k_scatter_adj<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, rowstart.p, off4.p, g->adj.p);
+  GARY_TRY(g->row.alloc_persistent(n));
+  GARY_TRY(g->indptr.alloc_persistent((uint64_t)n + 1));
+  k_row_records<<<grid_for((uint64_t)n + 1), kThreads, 0, s>>>(off4.p, dplus.p, n, g->row.p,
+                                                              g->indptr.p);
+  GARY_CUDA(cudaGetLastError());
+
+  // 8. statistics and per-vertex wedge counts
+  GARY_TRY(g->wedge.alloc_persistent(n));
+  GARY_CUDA(cudaMemsetAsync(g->wedge.p, 0, (uint64_t)n * 8, s));
+  if (m)
+    k_wedges<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, dplus.p,
+                                              reinterpret_cast<unsigned long long *>(g->wedge.p));
+  GARY_CUDA(cudaGetLastError());
+  g->max_out = thrust::reduce(pol, dplus.p, dplus.p + n, 0u, MaxU32());
+  g->out_deg_sq = thrust::transform_reduce(pol, dplus.p, dplus.p + n, Sq(), 0ull,
+                                           thrust::plus<uint64_t>());
+  g->wedges = thrust::reduce(pol, g->wedge.p, g->wedge.p + n, 0ull);
+  g->alg_bytes = 4 * g->out_deg_sq + 4 * g->wedges + 24 * g->m;
+  g->outdeg = std::move(dplus);
+  GARY_CUDA(cudaEventCreate(&g->ev0));
+  GARY_CUDA(cudaEventCreate(&g->ev1));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  *out = g.release();
+  return GARY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric CSR from an undirected edge list (dedup, drop loops, symmetrise).
+namespace {
+__global__ void k_edge_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                            uint64_t m, uint32_t n, int lg, uint64_t *__restrict__ keys,
+                            unsigned *err) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t a = src[i], b = dst[i];
+    if (a >= n || b >= n) {
+      atomicOr(err, kErrRange);
+      keys[2 * i] = keys[2 * i + 1] = ~0ull;
+    } else if (a == b) {
+      keys[2 * i] = keys[2 * i + 1] = ~0ull;
+    } else {
+      keys[2 * i] = ((uint64_t)a << lg) | b;
+      keys[2 * i + 1] = ((uint64_t)b << lg) | a;
+    }
+  }
+}
+__global__ void k_key_cols(const uint64_t *__restrict__ keys, uint64_t m, int lg,
+                           uint32_t *__restrict__ idx) {
+  const uint64_t mask = (1ull << lg) - 1;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    idx[i] = (uint32_t)(keys[i] & mask);
+}
+}  // namespace
+
+int csr_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_t n,
+                   uint32_t flags, cudaStream_t s, gary_csr **out) {
+  GARY_CHECK_ARG(out != nullptr, "out is NULL");
+  GARY_CHECK_ARG(n > 0 && n < 0xFFFFFFFFu, "n must be in [1, 2^32-1)");
+  GARY_CHECK_ARG(m == 0 || (src && dst), "src/dst is NULL");
+  *out = nullptr;
+  auto c = std::make_unique<gary_csr>();
+  GARY_CUDA(cudaGetDevice(&c->device));
+  c->n = n;
+  auto pol = thrust::cuda::par_nosync.on(s);
+  const int lg = bits_for(n);
+  DevBuf<uint32_t> s_own, d_own;
+  if (!(flags & GARY_INPUT_DEVICE) && m) {
+    GARY_TRY(s_own.alloc(m, s));
+    GARY_TRY(d_own.alloc(m, s));
+    GARY_CUDA(cudaMemcpyAsync(s_own.p, src, m * 4, cudaMemcpyHostToDevice, s));
+    GARY_CUDA(cudaMemcpyAsync(d_own.p, dst, m * 4, cudaMemcpyHostToDevice, s));
+    src = s_own.p;
+    dst = d_own.p;
+  }
+  DevBuf<unsigned> err;
+  GARY_TRY(err.alloc(1, s));
+  GARY_CUDA(cudaMemsetAsync(err.p, 0, 4, s));
+  DevBuf<uint64_t> keys, alt;
+  uint64_t k = 0;
+  GARY_TRY(keys.alloc(std::max<uint64_t>(2 * m, 1), s));
+  if (m) {
+    k_edge_keys<<<grid_for(m), kThreads, 0, s>>>(src, dst, m, n, lg, keys.p, err.p);
+    GARY_CUDA(cudaGetLastError());
+    k = thrust::remove(pol, keys.p, keys.p + 2 * m, ~0ull) - keys.p;
+  }
+  s_own.release();
+  d_own.release();
+  unsigned herr = 0;
+  GARY_TRY(read_err(err.p, s, &herr));
+  if (herr) return input_error(herr);
+  GARY_TRY(alt.alloc(std::max<uint64_t>(k, 1), s));
+  if (k) {
+    GARY_TRY(radix_sort_keys(keys, alt, k, 2 * lg, s));
+    k = thrust::unique(pol, keys.p, keys.p + k) - keys.p;
+  }
+  alt.release();
+  DevBuf<uint64_t> rowstart;
+  GARY_TRY(row_starts(keys, k, n, lg, rowstart, s, true));
+  GARY_TRY(c->idx.alloc_persistent(std::max<uint64_t>(k, 1)));
+  if (k) k_key_cols<<<grid_for(k), kThreads, 0, s>>>(keys.p, k, lg, c->idx.p);
+  GARY_CUDA(cudaGetLastError());
+  c->ptr = std::move(rowstart);
+  c->nnz = k;
+  GARY_CUDA(cudaStreamSynchronize(s));
+  *out = c.release();
+  return GARY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Unpadded host copies and the COO view.
+namespace {
+// heads for the padded layout: rowid of every padded word (kSentinel padding
+// words are dropped afterwards)
+__global__ void k_padded_heads(const uint2 *__restrict__ row, uint32_t n,
+                               uint32_t *__restrict__ rowid) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    uint2 r = row[u];
+    if (r.y) rowid[(uint64_t)r.x * 4] = (uint32_t)u;
+  }
+}
+struct IsReal {
+  const uint32_t *adj;
+  __host__ __device__ bool operator()(uint64_t w) const { return adj[w] != kSentinel; }
+};
+__global__ void k_gather_pairs(const uint64_t *__restrict__ words, uint64_t m,
+                               const uint32_t *__restrict__ rowid, const uint32_t *__restrict__ adj,
+                               uint32_t *__restrict__ r, uint32_t *__restrict__ c) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t w = words[i];
+    r[i] = rowid[w];
+    c[i] = adj[w];
+  }
+}
+}  // namespace
+
+int build_coo(gary_graph *g, cudaStream_t s) {
+  if (g->coo_row.p || g->m == 0) return GARY_OK;
+  auto pol = thrust::cuda::par_nosync.on(s);
+  DevBuf<uint32_t> rowid;
+  GARY_TRY(rowid.alloc(g->adj_words, s));
+  GARY_CUDA(cudaMemsetAsync(rowid.p, 0, g->adj_words * 4, s));
+  k_padded_heads<<<grid_for(g->n), kThreads, 0, s>>>(g->row.p, g->n, rowid.p);
+  {
+    size_t tmp = 0;
+    GARY_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp, rowid.p, rowid.p, MaxU32(),
+                                             g->adj_words, s));
+    DevBuf<uint8_t> t;
+    GARY_TRY(t.alloc(tmp, s));
+    GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), g->adj_words, s));
+  }
+  DevBuf<uint64_t> words;
+  GARY_TRY(words.alloc(g->m, s));
+  uint64_t got = thrust::copy_if(pol, thrust::counting_iterator<uint64_t>(0),
+                                 thrust::counting_iterator<uint64_t>(g->adj_words), words.p,
+                                 IsReal{g->adj.p}) - words.p;
+  if (got != g->m) {
+    set_error("internal: padded adjacency holds %llu ids, expected %llu",
+              (unsigned long long)got, (unsigned long long)g->m);
+    return GARY_ERR_CUDA;
+  }
+  GARY_TRY(g->coo_row.alloc_persistent(g->m));
+  GARY_TRY(g->coo_col.alloc_persistent(g->m));
+  k_gather_pairs<<<grid_for(g->m), kThreads, 0, s>>>(words.p, g->m, rowid.p, g->adj.p,
+                                                     g->coo_row.p, g->coo_col.p);
+  GARY_CUDA(cudaGetLastError());
+  GARY_CUDA(cudaStreamSynchronize(s));
+  return GARY_OK;
+}
+
+int download(gary_graph *g, uint64_t *ptr, uint32_t *idx, uint32_t *perm, cudaStream_t s) {
+  GARY_TRY(build_coo(g, s));
+  std::vector<uint32_t> deg(g->n);
+  GARY_CUDA(cudaMemcpyAsync(deg.data(), g->outdeg.p, (uint64_t)g->n * 4, cudaMemcpyDeviceToHost, s));
+  if (idx && g->m)
+    GARY_CUDA(cudaMemcpyAsync(idx, g->coo_col.p, g->m * 4, cudaMemcpyDeviceToHost, s));
+  if (perm) {
+    if (g->relabeled) {
+      GARY_CUDA(cudaMemcpyAsync(perm, g->perm.p, (uint64_t)g->n * 4, cudaMemcpyDeviceToHost, s));
+    } else {
+      for (uint32_t i = 0; i < g->n; ++i) perm[i] = i;
+    }
+  }
+  GARY_CUDA(cudaStreamSynchronize(s));
+  if (ptr) {
+    ptr[0] = 0;
+    for (uint32_t v = 0; v < g->n; ++v) ptr[v + 1] = ptr[v] + deg[v];
+  }
+  return GARY_OK;
+}
+
+int csr_download(const gary_csr *c, uint64_t *ptr, uint32_t *idx) {
+  if (ptr) GARY_CUDA(cudaMemcpy(ptr, c->ptr.p, ((uint64_t)c->n + 1) * 8, cudaMemcpyDeviceToHost));
+  if (idx && c->nnz) GARY_CUDA(cudaMemcpy(idx, c->idx.p, c->nnz * 4, cudaMemcpyDeviceToHost));
+  return GARY_OK;
+}
+
+}  // namespace gary
+
+// C-ABI entry points for the CSR builder live here with the struct definition.
+extern "C" int gary_csr_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m,
+                                   uint32_t n, uint32_t flags, void *stream, gary_csr **out) {
+  gary::clear_error();
+  try {
+    return gary::csr_from_edges(src, dst, m, n, flags, gary::as_stream(stream), out);
+  } catch (const std::bad_alloc &) {
+    gary::set_error("out of memory building the CSR");
+    return GARY_ERR_OOM;
+  } catch (const std::exception &e) {
+    gary::set_error("csr_from_edges: %s", e.what());
+    return GARY_ERR_CUDA;
+  }
+}
+
+extern "C" int gary_csr_info(const gary_csr *c, uint32_t *n, uint64_t *nnz) {
+  GARY_CHECK_ARG(c != nullptr, "csr is NULL");
+  if (n) *n = c->n;
+  if (nnz) *nnz = c->nnz;
+  return GARY_OK;
+}
+
+extern "C" int gary_csr_device_ptrs(const gary_csr *c, const uint64_t **ptr, const uint32_t **idx) {
+  GARY_CHECK_ARG(c != nullptr, "csr is NULL");
+  if (ptr) *ptr = c->ptr.p;
+  if (idx) *idx = c->idx.p;
+  return GARY_OK;
+}
+
+extern "C" int gary_csr_download(const gary_csr *c, uint64_t *ptr, uint32_t *idx) {
+  GARY_CHECK_ARG(c != nullptr, "csr is NULL");
+  gary::clear_error();
+  return gary::csr_download(c, ptr, idx);
+}
+
+extern "C" int gary_csr_free(gary_csr *c) {
+  if (!c) return GARY_OK;
+  delete c;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    gary::set_error("gary_csr_free: %s", cudaGetErrorString(e));
+    return GARY_ERR_CUDA;
+  }
+  return GARY_OK;
+}

@@ -1,0 +1,148 @@
+// Warp-cooperative building blocks shared by the counting and set-operation
+// kernels.  They restate, B200-first, what include/ops/{Search,Intersection}.cuh
+// of the reference provide:
+//   - shared-memory hash sets probed by every lane (the replacement for
+//     per-key global binary searches, Intersection.cuh:56-71);
+//   - a flattened ("load-balanced") walk over many short lists so that all 32
+//     lanes stay busy when lists are shorter than a warp (the reference idles
+//     lanes beyond |sA|, Intersection.cuh:130);
+//   - the two-phase cached binary search (Search.cuh:93-138) with a larger,
+//     CTA-wide sample cache and 64-bit index arithmetic (the reference's int32
+//     `i*size/N` overflows for lists >= 2^26, Intersection.cuh:256,291).
+#pragma once
+#include <cstdint>
+
+#include "internal.cuh"
+
+namespace gary {
+
+constexpr uint32_t kHashMul = 0x9E3779B1u;  // Fibonacci hashing
+
+__device__ __forceinline__ uint32_t hash_slot(uint32_t x, uint32_t shift) {
+  return (x * kHashMul) >> shift;
+}
+
+// log2 of the table size for `items` keys: T >= 2*items, T >= 32.
+__device__ __forceinline__ int hash_log2(uint32_t items) {
+  int l = items > 1 ? 32 - __clz(2 * items - 1) : 1;
+  return l < 5 ? 5 : l;
+}
+
+// Insert distinct keys keys[lo..hi) into an open-addressing table (linear
+// probing).  Every thread of the calling group takes a stride of the keys.
+__device__ __forceinline__ void hash_insert_range(uint32_t *tab, int logT, const uint32_t *keys,
+                                                  uint32_t lo, uint32_t hi, uint32_t tid,
+                                                  uint32_t nthreads) {
+  const uint32_t mask = (1u << logT) - 1, shift = 32 - logT;
+  for (uint32_t i = lo + tid; i < hi; i += nthreads) {
+    uint32_t x = keys[i];
+    uint32_t h = hash_slot(x, shift);
+    while (atomicCAS(&tab[h], kSentinel, x) != kSentinel) h = (h + 1) & mask;
+  }
+}
+
+__device__ __forceinline__ uint32_t hash_contains(const uint32_t *tab, int logT, uint32_t x) {
+  const uint32_t mask = (1u << logT) - 1;
+  uint32_t h = hash_slot(x, 32 - logT);
+  while (true) {
+    uint32_t t = tab[h];
+    if (t == x) return 1;
+    if (t == kSentinel) return 0;
+    h = (h + 1) & mask;
+  }
+}
+
+// Lowest lane index k with incl_k > p, for a non-decreasing per-lane
+// inclusive prefix `incl` (all 32 lanes must call).  5 shuffles.
+__device__ __forceinline__ int warp_owner(uint32_t incl, uint32_t p) {
+  int lo = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    uint32_t val = __shfl_sync(kFull, incl, lo + step - 1);
+    if (val <= p) lo += step;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t warp_inclusive_sum(uint32_t x, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(kFull, x, o);
+    if (lane >= o) x += t;
+  }
+  return x;
+}
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
+}
+
+// For the lists N+(v) of v = keys[j], j in the chunks jb, jb+jstep, ... < je
+// (each chunk 32 wide), count the members that `probe(w)` accepts.  The 32
+// lanes walk the concatenation of a chunk's lists, so short lists do not idle
+// lanes.  All 32 lanes must call.  Returns the per-lane count.
+template <typename Probe>
+__device__ __forceinline__ uint32_t warp_walk_lists(const GraphView &g, const uint32_t *keys,
+                                                    uint32_t jb, uint32_t je, uint32_t jstep,
+                                                    int lane, Probe probe) {
+  uint32_t cnt = 0;
+  for (uint32_t j = jb; j < je; j += jstep) {
+    const uint32_t jj = j + lane;
+    uint32_t len = 0, base = 0;
+    if (jj < je) {
+      const uint2 r = g.row[keys[jj]];
+      base = r.x;
+      len = r.y;
+    }
+    const uint32_t incl = warp_inclusive_sum(len, lane);
+    const uint32_t excl = incl - len;
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    for (uint32_t pb = 0; pb < total; pb += 32) {
+      const uint32_t p = pb + lane;
+      const int k = warp_owner(incl, p);
+      const uint32_t ek = __shfl_sync(kFull, excl, k);
+      const uint32_t bk = __shfl_sync(kFull, base, k);
+      if (p < total) cnt += probe(g.adj[(uint64_t)bk * 4 + (p - ek)]);
+    }
+  }
+  return cnt;
+}
+
+// Two-phase search (Search.cuh:120-138 restated): `cache` holds S samples
+// cache[i] = list[i*len/S] (i < S) -- or the whole list when len <= S, in
+// which case phase 2 never runs.  Returns 1 when x is in list.
+__device__ __forceinline__ uint32_t search_2phase(const uint32_t *list, uint32_t len,
+                                                  const uint32_t *cache, uint32_t S, uint32_t x) {
+  const uint32_t C = len <= S ? len : S;
+  // phase 1: last index with cache[i] <= x
+  int lo = 0, hi = (int)C - 1, pos = -1;
+  while (lo <= hi) {
+    int mid = (lo + hi) >> 1;
+    uint32_t v = cache[mid];
+    if (v == x) return 1;
+    if (v < x) {
+      pos = mid;
+      lo = mid + 1;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  if (len <= S || pos < 0) return 0;
+  // phase 2: list[(pos)*len/S + 1, (pos+1)*len/S) in global memory
+  uint64_t b = (uint64_t)pos * len / S + 1;
+  uint64_t e = (uint64_t)(pos + 1) * len / S;
+  while (b < e) {
+    uint64_t mid = (b + e) >> 1;
+    uint32_t v = list[mid];
+    if (v == x) return 1;
+    if (v < x)
+      b = mid + 1;
+    else
+      e = mid;
+  }
+  return 0;
+}
+
+}  // namespace gary

@@ -1,0 +1,184 @@
+/*
+ * gary_b200.h -- C ABI of the B200 subgraph-counting path.
+ *
+ * The reference (hirayaku/Gary) exposes this path only as C++ templates:
+ *   - DeviceGraphCtx / DeviceCSR / DeviceCOO / DeviceGraph
+ *       (include/DeviceGraph.cuh:15-133, src/DeviceGraph.cu:14-96)
+ *   - graph_query::triangleCountHom / triangleCountLegacy / getIndexCacheSMem
+ *       (include/kernels/GraphQueryHom.cuh:13-48, src/GraphQueryHom.cu:11-38)
+ *   - the warp-cooperative set operations of include/ops/{Search,Intersection}.cuh
+ * Each entry point below names the reference interface it replaces.  The C++
+ * shims in include/gary/ keep the reference's names on top of this ABI.
+ *
+ * Conventions
+ *   - every function returns an int status: GARY_OK (0) or a negative
+ *     GARY_ERR_* class; gary_last_error() describes the last failure of the
+ *     calling thread.  No C++ exception crosses this boundary.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Calls that return a host value synchronise that stream.
+ *   - vertex ids are uint32 (< 2^32 - 1; UINT32_MAX is the list padding
+ *     sentinel), edge offsets uint64.  The reference uses int32 / int64
+ *     (include/Defines.h:9-10); for every id below 2^31 the order and the
+ *     arithmetic are the same.
+ *   - a gary_graph is used by one host thread at a time; distinct graphs may
+ *     be used concurrently.
+ */
+#ifndef GARY_B200_H
+#define GARY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GARY_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define GARY_OK 0
+#define GARY_ERR_INVALID (-1)     /* bad argument (null pointer, size, flag) */
+#define GARY_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define GARY_ERR_OOM (-3)         /* device or host allocation failed */
+#define GARY_ERR_INPUT (-4)       /* malformed graph: unsorted, duplicate, loop, id >= n */
+#define GARY_ERR_TIMEOUT (-5)     /* a bounded device wait expired (scheduler, TMA) */
+#define GARY_ERR_UNSUPPORTED (-6) /* valid request this build cannot serve */
+
+/* ---- flags for gary_graph_upload / gary_csr_from_edges ----------------- */
+#define GARY_INPUT_SYMMETRIC 0x0u /* CSR lists every undirected edge in both rows */
+#define GARY_INPUT_DAG 0x1u       /* CSR lists every undirected edge once (any orientation) */
+#define GARY_INPUT_DEVICE 0x2u    /* input pointers are device pointers */
+#define GARY_KEEP_IDS 0x4u        /* orient by degree but keep caller vertex ids (no relabel) */
+#define GARY_VALIDATE 0x8u        /* check sortedness, range and self loops; GARY_ERR_INPUT */
+
+/* ---- patterns and schedulers for gary_count ---------------------------- */
+#define GARY_PATTERN_TRIANGLE 3 /* T = sum over oriented edges (u,v) of |N+(u) & N+(v)| */
+#define GARY_PATTERN_4CYCLE 4   /* non-induced 4-cycles, each counted once */
+#define GARY_PATTERN_4CLIQUE 5  /* 4-cliques, each counted once */
+
+#define GARY_SCHED_PLAIN 0   /* degree-threshold variant dispatch, work-based tile weights */
+#define GARY_SCHED_LEARNED 1 /* MLP cost model picks the variant and sets tile weights */
+
+/* ======================================================================== */
+const char *gary_last_error(void);
+int gary_abi_version(void);
+
+/* ---- device graph: replaces DeviceGraphCtx (include/DeviceGraph.cuh:75-133,
+ *      src/DeviceGraph.cu:14-96) ------------------------------------------ */
+typedef struct gary_graph gary_graph;
+
+typedef struct gary_graph_info {
+  uint32_t n;                /* vertices */
+  uint32_t max_degree;       /* max undirected degree */
+  uint32_t max_out_degree;   /* max oriented out-degree d+(u) */
+  uint32_t relabeled;        /* 1 when vertex ids are degree ranks */
+  uint64_t m;                /* undirected edges = |E+| */
+  uint64_t adj_words;        /* padded uint32 words of the oriented lists */
+  uint64_t wedges;           /* sum over (u,v) in E+ of d+(v) */
+  uint64_t out_deg_sq;       /* sum over u of d+(u)^2 */
+  uint64_t alg_bytes;        /* B_alg = sum over (u,v) in E+ of 4(d+(u)+d+(v)) + 24 */
+  uint64_t device_bytes;     /* bytes of device memory this graph holds */
+} gary_graph_info;
+
+/* Raw views with the reference's field names (include/DeviceGraph.cuh:15-67).
+ * colIdx + indPtr[v] points at v's oriented list, deg[v] entries long; lists
+ * start on 16-byte boundaries and are padded with UINT32_MAX.  The COO view
+ * has its own unpadded colIdx (the reference aliases the CSR's,
+ * DeviceGraph.cuh:117, which padding would break). */
+typedef struct gary_device_csr {
+  uint32_t m;
+  uint64_t nnz;
+  const uint64_t *indPtr;
+  const uint32_t *colIdx;
+  const uint32_t *deg;
+} gary_device_csr;
+
+typedef struct gary_device_coo {
+  uint32_t m;
+  uint64_t nnz;
+  const uint32_t *rowIdx;
+  const uint32_t *colIdx;
+  const uint32_t *deg;
+} gary_device_coo;
+
+/* Upload a CSR and build the degree-oriented, 16-byte-aligned, padded uint32
+ * lists on the device.  Replaces DeviceGraphCtx::loadFromHost(GraphCSR)
+ * (src/DeviceGraph.cu:18-28) plus the host orientation pass
+ * (src/Graph.cpp:34-61, convert.cpp:61-78).  Orientation is by (degree, id),
+ * not by id: triangle and clique counts do not depend on the order.
+ * ptr has n+1 entries, idx has nnz entries; lists sorted ascending, no
+ * duplicates, no self loops. */
+int gary_graph_upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz,
+                      uint32_t flags, void *stream, gary_graph **out);
+
+/* Replaces DeviceGraphCtx::clear() (src/DeviceGraph.cu:54-61). NULL is a no-op. */
+int gary_graph_free(gary_graph *g);
+
+int gary_graph_get_info(const gary_graph *g, gary_graph_info *out);
+
+/* Replaces DeviceGraphCtx::getDeviceCSR / getDeviceCOO (include/DeviceGraph.cuh:100-121).
+ * The COO arrays are built on first use, like the reference's lazy rowIdx. */
+int gary_graph_device_csr(gary_graph *g, gary_device_csr *out);
+int gary_graph_device_coo(gary_graph *g, gary_device_coo *out);
+
+/* Host copy of the oriented CSR without padding: ptr[n+1], idx[m].  With
+ * relabel on, ids are degree ranks; perm (may be NULL) receives rank -> caller id.
+ * Replaces DeviceGraphCtx::getHostCSR (src/DeviceGraph.cu:63-81). */
+int gary_graph_download(gary_graph *g, uint64_t *ptr, uint32_t *idx, uint32_t *perm);
+
+/* ---- counting: replaces graph_query::triangleCountHom<useCache,N,Policy>
+ *      (include/kernels/GraphQueryHom.cuh:15-43) and triangleCountLegacy
+ *      (src/GraphQueryHom.cu:15-38); 4-cycle / 4-clique have no reference
+ *      implementation (rectCountHom is declared only, GraphQueryHom.cuh:48). */
+
+/* Count `pattern` and write the uint64 total to *out (host).  Synchronises. */
+int gary_count(gary_graph *g, int pattern, int sched, void *stream, uint64_t *out);
+
+/* Same, asynchronous: the total is written to the device word *d_out (which
+ * the call zeroes first, unlike the reference, whose caller must zero it,
+ * test/TriQueryTest.cu:117).  No host synchronisation. */
+int gary_count_async(gary_graph *g, int pattern, int sched, void *stream, uint64_t *d_out);
+
+/* One shard of the count: every rank holds the whole graph and counts tile
+ * ranges [shard/nshards, (shard+1)/nshards) of the plan; the shard totals sum
+ * to the full count.  No reference counterpart (the reference is single-GPU,
+ * src/DeviceGraph.cu:91-96). */
+int gary_count_shard_async(gary_graph *g, int pattern, int sched, uint32_t shard,
+                           uint32_t nshards, void *stream, uint64_t *d_out);
+
+/* Statistics of the last gary_count* on g: kernel time of the counting kernel
+ * in milliseconds (CUDA events on its stream; call after that stream is
+ * synchronised), tiles, and the variant histogram (hash, search, merge,
+ * bitmap).  For benches. */
+typedef struct gary_count_stats {
+  float kernel_ms;
+  uint32_t tiles;
+  uint32_t cta_tiles;
+  uint32_t variant_tiles[4];
+} gary_count_stats;
+int gary_count_last_stats(gary_graph *g, gary_count_stats *out);
+
+/* ---- symmetric CSR construction on the device ------------------------- *
+ * Dedup, drop self loops, symmetrise and sort an undirected edge list into a
+ * CSR (the reference does this on the host: src/Graph.cpp:19-32, 63-91). */
+typedef struct gary_csr gary_csr;
+int gary_csr_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_t n,
+                        uint32_t flags, void *stream, gary_csr **out);
+int gary_csr_info(const gary_csr *c, uint32_t *n, uint64_t *nnz);
+int gary_csr_device_ptrs(const gary_csr *c, const uint64_t **ptr, const uint32_t **idx);
+int gary_csr_download(const gary_csr *c, uint64_t *ptr, uint32_t *idx);
+int gary_csr_free(gary_csr *c);
+
+/* ---- seeded synthetic generators (host; RMAT also on the device) ------ *
+ * Counter-based: edge i depends only on (seed, i), so any range can be
+ * regenerated on the host to check a device batch. */
+int gary_gen_er(uint32_t n, uint64_t m, uint64_t seed, uint32_t *src, uint32_t *dst);
+int gary_gen_rmat(int scale, uint64_t seed, uint64_t first, uint64_t count, uint32_t *src,
+                  uint32_t *dst);
+int gary_gen_rmat_device(int scale, uint64_t seed, uint64_t first, uint64_t count,
+                         uint32_t *d_src, uint32_t *d_dst, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GARY_B200_H */

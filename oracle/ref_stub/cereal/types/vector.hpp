@@ -1,0 +1,3 @@
+// cereal stub: see archives/binary.hpp
+#pragma once
+#include <vector>
