@@ -49,7 +49,7 @@ int sm_count() {
 
 int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
            cudaStream_t s, gary_graph **out);
-int build_coo(gary_graph *g, cudaStream_t s);
+int build_coo(PaddedCSR &c, cudaStream_t s);
 int download(gary_graph *g, uint64_t *ptr, uint32_t *idx, uint32_t *perm, cudaStream_t s);
 
 void free_plans(gary_graph *g) {
@@ -95,8 +95,8 @@ int count_async(gary_graph *g, int pattern, int sched, cudaStream_t s, unsigned 
     return GARY_ERR_UNSUPPORTED;
   }
   const int slot = plan_slot(pattern, sched);
-  if (!g->plans[slot]) GARY_TRY(build_plain_plan(g, PlanParams{}, s, &g->plans[slot]));
-  return launch_plain_k3(g, g->plans[slot], d_out, s, shard, nshards);
+  if (!g->plans[slot]) GARY_TRY(build_k3_plan(g, PlanParams{}, s, &g->plans[slot]));
+  return launch_k3(g, g->plans[slot], d_out, s, shard, nshards);
 }
 
 }  // namespace
@@ -135,10 +135,10 @@ extern "C" int gary_graph_get_info(const gary_graph *g, gary_graph_info *out) {
   GARY_CHECK_ARG(g != nullptr && out != nullptr, "NULL argument");
   out->n = g->n;
   out->max_degree = g->max_degree;
-  out->max_out_degree = g->max_out;
-  out->relabeled = g->relabeled ? 1u : 0u;
-  out->m = g->m;
-  out->adj_words = g->adj_words;
+  out->max_out_degree = g->dag.max_len;
+  out->relabeled = g->keep_ids ? 0u : 1u;
+  out->m = g->dag.m;
+  out->adj_words = g->dag.words;
   out->wedges = g->wedges;
   out->out_deg_sq = g->out_deg_sq;
   out->alg_bytes = g->alg_bytes;
@@ -148,23 +148,25 @@ extern "C" int gary_graph_get_info(const gary_graph *g, gary_graph_info *out) {
 
 extern "C" int gary_graph_device_csr(gary_graph *g, gary_device_csr *out) {
   GARY_CHECK_ARG(g != nullptr && out != nullptr, "NULL argument");
+  gary::PaddedCSR &c = g->user_view();
   out->m = g->n;
-  out->nnz = g->m;
-  out->indPtr = g->indptr.p;
-  out->colIdx = g->adj.p;
-  out->deg = g->outdeg.p;
+  out->nnz = c.m;
+  out->indPtr = c.indptr.p;
+  out->colIdx = c.adj.p;
+  out->deg = c.outdeg.p;
   return GARY_OK;
 }
 
 extern "C" int gary_graph_device_coo(gary_graph *g, gary_device_coo *out) {
   GARY_CHECK_ARG(g != nullptr && out != nullptr, "NULL argument");
   return guarded("gary_graph_device_coo", [&] {
-    GARY_TRY(gary::build_coo(g, nullptr));
+    gary::PaddedCSR &c = g->user_view();
+    GARY_TRY(gary::build_coo(c, nullptr));
     out->m = g->n;
-    out->nnz = g->m;
-    out->rowIdx = g->coo_row.p;
-    out->colIdx = g->coo_col.p;
-    out->deg = g->outdeg.p;
+    out->nnz = c.m;
+    out->rowIdx = c.coo_row.p;
+    out->colIdx = c.coo_col.p;
+    out->deg = c.outdeg.p;
     return GARY_OK;
   });
 }

@@ -264,12 +264,65 @@ int input_error(unsigned bits) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Padded lists from sorted (row << lg | col) keys.
+int padded_from_keys(const DevBuf<uint64_t> &keys, uint64_t m, uint32_t n, int lg, PaddedCSR &c,
+                     cudaStream_t s) {
+  auto pol = thrust::cuda::par_nosync.on(s);
+  c.n = n;
+  c.m = m;
+  DevBuf<uint64_t> rowstart, off4;
+  GARY_TRY(row_starts(keys, m, n, lg, rowstart, s));
+  GARY_TRY(c.outdeg.alloc_persistent(n));
+  GARY_TRY(off4.alloc((uint64_t)n + 1, s));
+  k_rows<<<grid_for(n), kThreads, 0, s>>>(rowstart.p, n, c.outdeg.p, off4.p);
+  thrust::exclusive_scan(pol, off4.p, off4.p + n + 1, off4.p, 0ull);
+  uint64_t quads = 0;
+  GARY_CUDA(cudaMemcpyAsync(&quads, off4.p + n, 8, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  if (quads >= (1ull << 32)) {
+    set_error("graph too large: %llu padded words", (unsigned long long)quads * 4);
+    return GARY_ERR_UNSUPPORTED;
+  }
+  c.words = quads * 4;
+  GARY_TRY(c.adj.alloc_persistent(std::max<uint64_t>(c.words, 4)));
+  GARY_CUDA(cudaMemsetAsync(c.adj.p, 0xFF, c.adj.bytes(), s));
+  if (m) k_scatter_adj<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, rowstart.p, off4.p, c.adj.p);
+  GARY_TRY(c.row.alloc_persistent(n));
+  GARY_TRY(c.indptr.alloc_persistent((uint64_t)n + 1));
+  k_row_records<<<grid_for((uint64_t)n + 1), kThreads, 0, s>>>(off4.p, c.outdeg.p, n, c.row.p,
+                                                              c.indptr.p);
+  GARY_CUDA(cudaGetLastError());
+  c.max_len = thrust::reduce(pol, c.outdeg.p, c.outdeg.p + n, 0u, MaxU32());
+  return GARY_OK;
+}
+
+// Oriented keys of every CSR entry, compacted and sorted.  rank == nullptr:
+// caller ids; else degree ranks.
+int oriented_keys(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz, uint32_t n,
+                  const uint32_t *deg, const uint32_t *rank, int lg, bool dag, bool validate,
+                  unsigned *err, DevBuf<uint64_t> &keys, uint64_t &m, cudaStream_t s) {
+  auto pol = thrust::cuda::par_nosync.on(s);
+  m = 0;
+  GARY_TRY(keys.alloc(std::max<uint64_t>(nnz, 1), s));
+  if (nnz) {
+    k_make_keys<<<grid_for(nnz), kThreads, 0, s>>>(rowid, didx, nnz, n, deg, rank, lg, dag,
+                                                   validate, keys.p, err);
+    GARY_CUDA(cudaGetLastError());
+    m = thrust::remove(pol, keys.p, keys.p + nnz, ~0ull) - keys.p;
+  }
+  DevBuf<uint64_t> alt;
+  GARY_TRY(alt.alloc(std::max<uint64_t>(m, 1), s));
+  if (m) GARY_TRY(radix_sort_keys(keys, alt, m, 2 * lg, s));
+  return GARY_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Oriented upload.  Input CSR (symmetric or DAG) -> degree-oriented padded lists.
 int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
            cudaStream_t s, gary_graph **out) {
   const bool on_dev = flags & GARY_INPUT_DEVICE;
   const bool dag = flags & GARY_INPUT_DAG;
-  const bool relabel = !(flags & GARY_KEEP_IDS);
+  const bool keep_ids = flags & GARY_KEEP_IDS;
   const bool validate = flags & GARY_VALIDATE;
   GARY_CHECK_ARG(out != nullptr, "out is NULL");
   GARY_CHECK_ARG(n > 0 && n < 0xFFFFFFFFu, "n must be in [1, 2^32-1)");
@@ -284,7 +337,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   GARY_CUDA(cudaGetDevice(&g->device));
   g->n = n;
   g->flags = flags;
-  g->relabeled = relabel;
+  g->keep_ids = keep_ids;
   auto pol = thrust::cuda::par_nosync.on(s);
 
   // 1. input on the device
@@ -321,9 +374,9 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   }
   g->max_degree = thrust::reduce(pol, deg.p, deg.p + n, 0u, MaxU32());
 
-  // 3. relabel: rank by (degree, id) with a stable radix sort on degree
+  // 3. ranks by (degree, id): a stable radix sort of the ids on degree
   DevBuf<uint32_t> rank;
-  if (relabel) {
+  {
     DevBuf<uint32_t> dk, dk2, perm2;
     GARY_TRY(dk.alloc(n, s));
     GARY_TRY(dk2.alloc(n, s));
@@ -346,88 +399,52 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
 
   // 4. row id of every entry: heads, then an inclusive max-scan
   const int lg = bits_for(n);
+  DevBuf<uint32_t> rowid;
+  GARY_TRY(rowid.alloc(nnz, s));
+  if (nnz) {
+    GARY_CUDA(cudaMemsetAsync(rowid.p, 0, nnz * 4, s));
+    k_row_heads<<<grid_for(n), kThreads, 0, s>>>(dptr, n, rowid.p);
+    size_t tmp = 0;
+    GARY_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
+    DevBuf<uint8_t> t;
+    GARY_TRY(t.alloc(tmp, s));
+    GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
+  }
+
+  // 5. oriented, ranked keys: sorted, validated
   DevBuf<uint64_t> keys;
   uint64_t m = 0;
-  {
-    DevBuf<uint32_t> rowid;
-    GARY_TRY(rowid.alloc(nnz, s));
-    if (nnz) {
-      GARY_CUDA(cudaMemsetAsync(rowid.p, 0, nnz * 4, s));
-      k_row_heads<<<grid_for(n), kThreads, 0, s>>>(dptr, n, rowid.p);
-      size_t tmp = 0;
-      GARY_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
-      DevBuf<uint8_t> t;
-      GARY_TRY(t.alloc(tmp, s));
-      GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
-    }
-    // 5. oriented keys, compacted
-    GARY_TRY(keys.alloc(std::max<uint64_t>(nnz, 1), s));
-    if (nnz) {
-      k_make_keys<<<grid_for(nnz), kThreads, 0, s>>>(rowid.p, didx, nnz, n, deg.p,
-                                                     relabel ? rank.p : nullptr, lg, dag, validate,
-                                                     keys.p, err.p);
-      GARY_CUDA(cudaGetLastError());
-      m = thrust::remove(pol, keys.p, keys.p + nnz, ~0ull) - keys.p;
-    }
-  }
-  dptr_own.release();
-  didx_own.release();
+  GARY_TRY(oriented_keys(rowid.p, didx, nnz, n, deg.p, rank.p, lg, dag, validate, err.p, keys, m, s));
   unsigned herr = 0;
   GARY_TRY(read_err(err.p, s, &herr));
   if (herr) return input_error(herr);
   if (!dag && 2 * m != nnz) return input_error(kErrAsym);
-
-  // 6. sort (row, col) keys; validate uniqueness
-  {
-    DevBuf<uint64_t> alt;
-    GARY_TRY(alt.alloc(std::max<uint64_t>(m, 1), s));
-    if (m) GARY_TRY(radix_sort_keys(keys, alt, m, 2 * lg, s));
-  }
   if (validate || dag) {
     if (m > 1) k_check_unique<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, err.p);
     GARY_TRY(read_err(err.p, s, &herr));
     if (herr) return input_error(herr);
   }
-  g->m = m;
 
-  // 7. rows, padded offsets, adjacency
-  DevBuf<uint64_t> rowstart, off4;
-  DevBuf<uint32_t> dplus;
-  GARY_TRY(row_starts(keys, m, n, lg, rowstart, s));
-  GARY_TRY(dplus.alloc_persistent(n));
-  GARY_TRY(off4.alloc((uint64_t)n + 1, s));
-  k_rows<<<grid_for(n), kThreads, 0, s>>>(rowstart.p, n, dplus.p, off4.p);
-  thrust::exclusive_scan(pol, off4.p, off4.p + n + 1, off4.p, 0ull);
-  uint64_t quads = 0;
-  GARY_CUDA(cudaMemcpyAsync(&quads, off4.p + n, 8, cudaMemcpyDeviceToHost, s));
-  GARY_CUDA(cudaStreamSynchronize(s));
-  if (quads >= (1ull << 32)) {
-    set_error("graph too large: %llu padded words", (unsigned long long)quads * 4);
-    return GARY_ERR_UNSUPPORTED;
-  }
-  g->adj_words = quads * 4;
-  GARY_TRY(g->adj.alloc_persistent(std::max<uint64_t>(g->adj_words, 4)));
-  GARY_CUDA(cudaMemsetAsync(g->adj.p, 0xFF, g->adj.bytes(), s));
-  if (m) k_scatter_adj<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, rowstart.p, off4.p, g->adj.p);
-  GARY_TRY(g->row.alloc_persistent(n));
-  GARY_TRY(g->indptr.alloc_persistent((uint64_t)n + 1));
-  k_row_records<<<grid_for((uint64_t)n + 1), kThreads, 0, s>>>(off4.p, dplus.p, n, g->row.p,
-                                                              g->indptr.p);
-  GARY_CUDA(cudaGetLastError());
-
-  // 8. statistics and per-vertex wedge counts
+  // 6. the kernels' padded lists, per-vertex wedge counts, statistics
+  GARY_TRY(padded_from_keys(keys, m, n, lg, g->dag, s));
   GARY_TRY(g->wedge.alloc_persistent(n));
   GARY_CUDA(cudaMemsetAsync(g->wedge.p, 0, (uint64_t)n * 8, s));
   if (m)
-    k_wedges<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, dplus.p,
+    k_wedges<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, g->dag.outdeg.p,
                                               reinterpret_cast<unsigned long long *>(g->wedge.p));
   GARY_CUDA(cudaGetLastError());
-  g->max_out = thrust::reduce(pol, dplus.p, dplus.p + n, 0u, MaxU32());
-  g->out_deg_sq = thrust::transform_reduce(pol, dplus.p, dplus.p + n, Sq(), 0ull,
+  g->out_deg_sq = thrust::transform_reduce(pol, g->dag.outdeg.p, g->dag.outdeg.p + n, Sq(), 0ull,
                                            thrust::plus<uint64_t>());
   g->wedges = thrust::reduce(pol, g->wedge.p, g->wedge.p + n, 0ull);
-  g->alg_bytes = 4 * g->out_deg_sq + 4 * g->wedges + 24 * g->m;
-  g->outdeg = std::move(dplus);
+  g->alg_bytes = 4 * g->out_deg_sq + 4 * g->wedges + 24 * m;
+  keys.release();
+
+  // 7. the same orientation in caller ids, for the views (GARY_KEEP_IDS)
+  if (keep_ids) {
+    uint64_t m2 = 0;
+    GARY_TRY(oriented_keys(rowid.p, didx, nnz, n, deg.p, nullptr, lg, dag, false, err.p, keys, m2, s));
+    GARY_TRY(padded_from_keys(keys, m2, n, lg, g->kept, s));
+  }
   GARY_CUDA(cudaEventCreate(&g->ev0));
   GARY_CUDA(cudaEventCreate(&g->ev1));
   GARY_CUDA(cudaStreamSynchronize(s));
@@ -547,48 +564,51 @@ __global__ void k_gather_pairs(const uint64_t *__restrict__ words, uint64_t m,
 }
 }  // namespace
 
-int build_coo(gary_graph *g, cudaStream_t s) {
-  if (g->coo_row.p || g->m == 0) return GARY_OK;
+int padded_rowid(const PaddedCSR &c, DevBuf<uint32_t> &rowid, cudaStream_t s) {
+  GARY_TRY(rowid.alloc(std::max<uint64_t>(c.words, 1), s));
+  if (!c.words) return GARY_OK;
+  GARY_CUDA(cudaMemsetAsync(rowid.p, 0, c.words * 4, s));
+  k_padded_heads<<<grid_for(c.n), kThreads, 0, s>>>(c.row.p, c.n, rowid.p);
+  size_t tmp = 0;
+  GARY_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp, rowid.p, rowid.p, MaxU32(), c.words, s));
+  DevBuf<uint8_t> t;
+  GARY_TRY(t.alloc(tmp, s));
+  GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), c.words, s));
+  return GARY_OK;
+}
+
+int build_coo(PaddedCSR &c, cudaStream_t s) {
+  if (c.coo_row.p || c.m == 0) return GARY_OK;
   auto pol = thrust::cuda::par_nosync.on(s);
   DevBuf<uint32_t> rowid;
-  GARY_TRY(rowid.alloc(g->adj_words, s));
-  GARY_CUDA(cudaMemsetAsync(rowid.p, 0, g->adj_words * 4, s));
-  k_padded_heads<<<grid_for(g->n), kThreads, 0, s>>>(g->row.p, g->n, rowid.p);
-  {
-    size_t tmp = 0;
-    GARY_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp, rowid.p, rowid.p, MaxU32(),
-                                             g->adj_words, s));
-    DevBuf<uint8_t> t;
-    GARY_TRY(t.alloc(tmp, s));
-    GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), g->adj_words, s));
-  }
+  GARY_TRY(padded_rowid(c, rowid, s));
   DevBuf<uint64_t> words;
-  GARY_TRY(words.alloc(g->m, s));
+  GARY_TRY(words.alloc(c.m, s));
   uint64_t got = thrust::copy_if(pol, thrust::counting_iterator<uint64_t>(0),
-                                 thrust::counting_iterator<uint64_t>(g->adj_words), words.p,
-                                 IsReal{g->adj.p}) - words.p;
-  if (got != g->m) {
+                                 thrust::counting_iterator<uint64_t>(c.words), words.p,
+                                 IsReal{c.adj.p}) - words.p;
+  if (got != c.m) {
     set_error("internal: padded adjacency holds %llu ids, expected %llu",
-              (unsigned long long)got, (unsigned long long)g->m);
+              (unsigned long long)got, (unsigned long long)c.m);
     return GARY_ERR_CUDA;
   }
-  GARY_TRY(g->coo_row.alloc_persistent(g->m));
-  GARY_TRY(g->coo_col.alloc_persistent(g->m));
-  k_gather_pairs<<<grid_for(g->m), kThreads, 0, s>>>(words.p, g->m, rowid.p, g->adj.p,
-                                                     g->coo_row.p, g->coo_col.p);
+  GARY_TRY(c.coo_row.alloc_persistent(c.m));
+  GARY_TRY(c.coo_col.alloc_persistent(c.m));
+  k_gather_pairs<<<grid_for(c.m), kThreads, 0, s>>>(words.p, c.m, rowid.p, c.adj.p, c.coo_row.p,
+                                                    c.coo_col.p);
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaStreamSynchronize(s));
   return GARY_OK;
 }
 
 int download(gary_graph *g, uint64_t *ptr, uint32_t *idx, uint32_t *perm, cudaStream_t s) {
-  GARY_TRY(build_coo(g, s));
+  PaddedCSR &c = g->user_view();
+  GARY_TRY(build_coo(c, s));
   std::vector<uint32_t> deg(g->n);
-  GARY_CUDA(cudaMemcpyAsync(deg.data(), g->outdeg.p, (uint64_t)g->n * 4, cudaMemcpyDeviceToHost, s));
-  if (idx && g->m)
-    GARY_CUDA(cudaMemcpyAsync(idx, g->coo_col.p, g->m * 4, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaMemcpyAsync(deg.data(), c.outdeg.p, (uint64_t)g->n * 4, cudaMemcpyDeviceToHost, s));
+  if (idx && c.m) GARY_CUDA(cudaMemcpyAsync(idx, c.coo_col.p, c.m * 4, cudaMemcpyDeviceToHost, s));
   if (perm) {
-    if (g->relabeled) {
+    if (!g->keep_ids) {
       GARY_CUDA(cudaMemcpyAsync(perm, g->perm.p, (uint64_t)g->n * 4, cudaMemcpyDeviceToHost, s));
     } else {
       for (uint32_t i = 0; i < g->n; ++i) perm[i] = i;

@@ -103,10 +103,14 @@ struct DevBuf {
 // ---- kernel-side graph view: one 8-byte row record per vertex -----------
 // row[v] = {off4, len}: v's list starts at adj + 4*off4 (16-byte aligned) and
 // holds len ids, padded with kSentinel up to a multiple of 4.
+// ranked: ids are degree ranks, so every list is in orientation order and
+// N+(v) holds only ids > v.  Kernels use it to skip list prefixes that cannot
+// close a pattern; with caller ids (GARY_KEEP_IDS) they must not.
 struct GraphView {
   uint32_t n;
   const uint2 *__restrict__ row;
   const uint32_t *__restrict__ adj;
+  bool ranked;
 };
 
 // grid sizing helper: a multiple of the SM count

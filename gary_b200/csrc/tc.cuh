@@ -8,23 +8,26 @@
 namespace gary {
 
 constexpr int kTcWarps = 16;               // warps per CTA of the counting kernel
-constexpr uint32_t kWarpTableSlots = 1024;  // per-warp shared hash table (4 KB)
+constexpr uint32_t kWarpTableSlots = 1024;  // per-warp shared set (4 KB)
 constexpr uint32_t kGroupTile = 0xFFFFFFFFu;
 
 enum : uint8_t { kClassNone = 0, kClassLight = 1, kClassSplit = 2, kClassCta = 3 };
 
-// A unit of scheduled work.
-//   j1 == kGroupTile : every light vertex u in [u0, u1), whole lists
-//   otherwise        : vertex u0 only, middle vertices N+(u0)[j0..j1)
+// Intersection variants a tile can run (the cost model's output order).
+enum : uint32_t { kVarHash = 0, kVarSearch = 1, kVarMerge = 2, kVarBitmap = 3 };
+
+// A unit of scheduled work over middle vertices v.
+//   j1 == kGroupTile : every light vertex v in [v0, v1), all its in-edges
+//   otherwise        : vertex v0 only, in-edges [j0, j1) of its in-list
 struct Tile {
-  uint32_t u0, u1, j0, j1;
+  uint32_t v0, v1, j0, j1;
 };
 
 struct PlanParams {
-  uint32_t warp_cap = kWarpTableSlots / 2;  // largest d+(u) a warp table takes
-  uint64_t warp_tile_cost = 1u << 13;       // target work per warp tile
-  uint64_t cta_tile_cost = 1u << 17;        // target work per CTA tile
-  uint64_t vertex_overhead = 48;            // fixed cost of a vertex (row loads, table clear)
+  uint32_t warp_cap = kWarpTableSlots / 2;  // largest d+(v) a warp set takes
+  uint64_t warp_tile_cost = 1u << 15;       // target probes per warp tile
+  uint64_t cta_tile_cost = 1u << 20;        // target probes per CTA tile
+  uint64_t vertex_overhead = 64;            // fixed cost of a middle vertex
 };
 
 // Contiguous tile ranges of one shard (multi-GPU: every rank holds the whole
@@ -50,20 +53,32 @@ struct SchedState {
   uint32_t pad;
 };
 
+// In-edge index of the middle-vertex formulation.  For every oriented edge
+// u -> v whose list suffix after v is non-empty, and with d+(v) > 0:
+//   inedge[k] = {first word of N+(u) after v, length of that suffix}
+// grouped by v: v's records are inedge[inptr[v] .. inptr[v+1]).
+struct InIndex {
+  DevBuf<uint2> inedge;
+  DevBuf<uint64_t> inptr;
+  DevBuf<uint64_t> work;  // per v: sum of suffix lengths (probes)
+  uint64_t records = 0;
+  uint64_t total_work = 0;
+};
+
 }  // namespace gary
 
 struct gary_count_plan {
   gary::PlanParams params;
+  gary::InIndex in;
   gary::DevBuf<uint8_t> vclass;
   gary::DevBuf<gary::Tile> tiles;
   uint32_t n_cta = 0;
   uint32_t n_warp = 0;
   gary::DevBuf<gary::SchedState> sched;
-  gary::DevBuf<unsigned long long> result;
 };
 
 namespace gary {
-int build_plain_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_count_plan **out);
-int launch_plain_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out,
-                    cudaStream_t s, uint32_t shard, uint32_t nshards);
+int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_count_plan **out);
+int launch_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
+              uint32_t shard, uint32_t nshards);
 }  // namespace gary

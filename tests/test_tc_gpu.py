@@ -16,6 +16,14 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
+def _has_lib(name):
+    try:
+        C.CDLL(name)
+        return True
+    except OSError:
+        return False
+
+
 def _upload_host(ptr, idx, n, flags=0):
     return gb.Graph.upload(np.ascontiguousarray(ptr, np.uint64), np.ascontiguousarray(idx, np.uint32), n, flags)
 
@@ -113,9 +121,11 @@ def test_malformed_input_rejected(cuda):
     assert up([0, 2, 4, 6], [2, 1, 0, 2, 0, 1], 3) == _lib.GARY_ERR_INPUT       # unsorted
     assert up([0, 2, 4, 6], [0, 2, 0, 2, 0, 1], 3) == _lib.GARY_ERR_INPUT       # self loop
     assert up([0, 2, 4, 6], [1, 7, 0, 2, 0, 1], 3) == _lib.GARY_ERR_INPUT       # id >= n
-    assert up([0, 2, 3, 4], [1, 2, 0, 0], 3) == _lib.GARY_ERR_INPUT             # 1-2 one-way
-    assert up([0, 1, 1], [1, 1], 2, _lib.GARY_INPUT_DAG) == _lib.GARY_ERR_INPUT  # dup edge
+    assert up([0, 2, 4, 5], [1, 2, 0, 2, 0], 3) == _lib.GARY_ERR_INPUT          # 1->2 one-way
+    assert up([0, 1, 2, 3, 4], [1, 2, 3, 0], 4) == _lib.GARY_ERR_INPUT          # directed 4-cycle
+    assert up([0, 1, 2], [1, 0], 2, _lib.GARY_INPUT_DAG) == _lib.GARY_ERR_INPUT  # edge listed twice
     assert b"malformed" in _lib.load().gary_last_error()
+    assert up([0, 1, 1], [1, 1], 2, _lib.GARY_INPUT_DAG) == _lib.GARY_ERR_INVALID  # ptr[n] != nnz
 
 
 def test_empty_and_tiny(cuda):
@@ -150,13 +160,14 @@ def test_device_views(golden, cuda):
         coo = g.device_coo()
         assert csr.m == n and csr.nnz == len(i) and coo.nnz == len(i)
         # the views are raw device pointers: read them back through torch
+        cudart = C.CDLL("libcudart.so.12") if _has_lib("libcudart.so.12") else C.CDLL(
+            "/usr/local/cuda/lib64/libcudart.so")
+        cudart.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+
         def dev(ptr_, count, dt):
-            buf = (C.c_byte * (count * np.dtype(dt).itemsize))()
-            assert torch.cuda.is_available()
-            import ctypes
-            cudart = torch.cuda.cudart()
-            cudart.cudaMemcpy(ctypes.addressof(buf), ptr_, count * np.dtype(dt).itemsize, 2)
-            return np.frombuffer(buf, dt).copy()
+            out = np.empty(count, dt)
+            assert cudart.cudaMemcpy(out.ctypes.data, ptr_, out.nbytes, 2) == 0  # DeviceToHost
+            return out
         rows = dev(coo.rowIdx, len(i), np.uint32)
         cols = dev(coo.colIdx, len(i), np.uint32)
         assert np.array_equal(cols, i)
