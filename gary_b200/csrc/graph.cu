@@ -284,7 +284,8 @@ int padded_from_keys(const DevBuf<uint64_t> &keys, uint64_t m, uint32_t n, int l
     return GARY_ERR_UNSUPPORTED;
   }
   c.words = quads * 4;
-  GARY_TRY(c.adj.alloc_persistent(std::max<uint64_t>(c.words, 4)));
+  // 4 slack words: 32-byte-aligned octet reads of the last list stay in bounds
+  GARY_TRY(c.adj.alloc_persistent(c.words + 4));
   GARY_CUDA(cudaMemsetAsync(c.adj.p, 0xFF, c.adj.bytes(), s));
   if (m) k_scatter_adj<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, rowstart.p, off4.p, c.adj.p);
   GARY_TRY(c.row.alloc_persistent(n));

@@ -117,20 +117,28 @@ __global__ void k_in_work(const uint32_t *__restrict__ keys, const uint2 *__rest
   }
 }
 
-__global__ void k_classify(const uint2 *__restrict__ row, const uint64_t *__restrict__ work,
+__global__ void k_classify(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
+                           const uint64_t *__restrict__ work,
                            const uint64_t *__restrict__ inptr, uint32_t n, PlanParams pp,
                            uint8_t *__restrict__ vclass, uint64_t *__restrict__ costL,
                            uint32_t *__restrict__ kW, uint32_t *__restrict__ kC) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
        v += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t dv = row[v].y;
+    const uint2 rv = row[v];
+    const uint32_t dv = rv.y;
     const uint64_t nin = inptr[v + 1] - inptr[v];
     uint8_t cls = kClassNone;
     uint64_t cl = 0;
     uint32_t kw = 0, kc = 0;
     if (dv && nin) {
-      const uint64_t c = work[v] + dv + pp.vertex_overhead;
-      if (dv > pp.warp_cap) {
+      // a warp holds N+(v) as a bitmap when its id span is short, else as
+      // buckets when d+(v) <= warp_cap; otherwise the CTA shares one set
+      const uint32_t span = adj[(uint64_t)rv.x * 4 + dv - 1] - adj[(uint64_t)rv.x * 4];
+      const bool bitmap = span <= bitmap_max_span(kWarpTableSlots);
+      const bool warp_fits = bitmap || dv <= pp.warp_cap;
+      const uint64_t build = bitmap ? (span >> 5) + dv : 4ull * dv;
+      const uint64_t c = work[v] + build + pp.vertex_overhead;
+      if (!warp_fits) {
         cls = kClassCta;
         kc = (uint32_t)min_u64((c + pp.cta_tile_cost - 1) / pp.cta_tile_cost, nin);
       } else if (c > pp.warp_tile_cost) {
@@ -257,7 +265,7 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
   GARY_TRY(costL.alloc((uint64_t)n + 1, s));
   GARY_TRY(kW.alloc((uint64_t)n + 1, s));
   GARY_TRY(kC.alloc((uint64_t)n + 1, s));
-  k_classify<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, plan->in.work.p, plan->in.inptr.p, n, pp,
+  k_classify<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, plan->in.work.p, plan->in.inptr.p, n, pp,
                                               plan->vclass.p, costL.p, kW.p, kC.p);
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaMemsetAsync(costL.p + n, 0, 8, s));
@@ -304,91 +312,80 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
 // Counting kernel
 namespace {
 
-// Shared-memory set of N+(v): a bitmap over [lo, lo + span] when the id
-// range is short enough, else an open-addressing hash table.
-struct MidSet {
-  const uint32_t *mem;
-  uint32_t lo, span;
-  int logT;  // 0: bitmap
-  __device__ __forceinline__ uint32_t contains(uint32_t x) const {
-    const uint32_t o = x - lo;
-    if (o > span) return 0;
-    if (logT == 0) return (mem[o >> 5] >> (o & 31)) & 1u;
-    return hash_contains(mem, logT, x);
-  }
-};
+constexpr uint32_t kWarpBitmapSpan = bitmap_max_span(kWarpTableSlots);  // ids a warp bitmap covers
 
-// Build the set with `nthreads` cooperating threads (a warp or the CTA) in
-// `slots` words of shared memory; `sync` separates clear, fill and use.
-template <typename Sync>
-__device__ __forceinline__ MidSet build_set(const uint32_t *__restrict__ av, uint32_t d,
-                                            uint32_t *mem, uint32_t slots, uint32_t tid,
-                                            uint32_t nthreads, Sync sync) {
-  MidSet st;
-  st.mem = mem;
-  st.lo = av[0];
-  st.span = av[d - 1] - st.lo;
-  if (st.span < slots * 32u) {
-    st.logT = 0;
-    const uint32_t words = (st.span >> 5) + 1;
-    for (uint32_t i = tid; i < words; i += nthreads) mem[i] = 0;
-    sync();
-    for (uint32_t i = tid; i < d; i += nthreads) {
-      const uint32_t o = av[i] - st.lo;
-      atomicOr(&mem[o >> 5], 1u << (o & 31));
-    }
-  } else {
-    const int l = 32 - __clz(4 * d - 1);  // T >= 4d: load factor <= 1/4 when it fits
-    const int cap = 31 - __clz(slots);
-    st.logT = l < 5 ? 5 : (l > cap ? cap : l);
-    for (uint32_t i = tid; i < (1u << st.logT); i += nthreads) mem[i] = kSentinel;
-    sync();
-    hash_insert_range(mem, st.logT, av, 0, d, tid, nthreads);
+// One chunk of at most 32 in-edge records [kb, ke): count the members of each
+// suffix that `set` holds.  Suffixes are read as 32-byte-aligned octets of
+// ids (two 16-byte loads from one sector; the padded layout plus 4 slack
+// words at the end of adj keep every octet in bounds); the lanes walk the
+// concatenation of the chunk's octets, so short suffixes do not idle lanes.
+// Ids of an octet outside the suffix are masked.  All 32 lanes must call.
+template <typename Set>
+__device__ __forceinline__ uint32_t walk_chunk(const uint4 *__restrict__ adj4,
+                                               const uint2 *__restrict__ edges, uint64_t kb,
+                                               uint64_t ke, int lane, const Set &set) {
+  const uint64_t kk = kb + lane;
+  uint32_t s = 0, e = 0, o0 = 0, no = 0;
+  if (kk < ke) {
+    const uint2 r = edges[kk];
+    s = r.x;
+    e = r.x + r.y;
+    o0 = s >> 3;
+    no = ((e + 7) >> 3) - o0;
   }
-  sync();
-  return st;
+  const uint32_t incl = warp_inclusive_sum(no, lane);
+  const uint32_t excl = incl - no;
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  uint32_t cnt = 0;
+  for (uint32_t pb = 0; pb < total; pb += 32) {
+    const uint32_t p = pb + lane;
+    const int o = warp_owner(incl, p);
+    const uint32_t ox = __shfl_sync(kFull, excl, o);
+    const uint32_t oo = __shfl_sync(kFull, o0, o);
+    const uint32_t os = __shfl_sync(kFull, s, o);
+    const uint32_t oe = __shfl_sync(kFull, e, o);
+    if (p < total) {
+      const uint32_t oc = oo + (p - ox);
+      const uint4 a = adj4[2 * oc];
+      const uint4 b = adj4[2 * oc + 1];
+      const uint32_t w = oc * 8;
+      // valid ids of this octet: words [max(w, os), min(w + 8, oe))
+      const uint32_t skip = os > w ? os - w : 0u;
+      const uint32_t keep = oe - w < 8u ? oe - w : 8u;
+      const uint32_t vm = ((1u << keep) - 1u) & ~((1u << skip) - 1u);
+      cnt += (set.contains(a.x) & vm) + (set.contains(a.y) & (vm >> 1)) +
+             (set.contains(a.z) & (vm >> 2)) + (set.contains(a.w) & (vm >> 3)) +
+             (set.contains(b.x) & (vm >> 4)) + (set.contains(b.y) & (vm >> 5)) +
+             (set.contains(b.z) & (vm >> 6)) + (set.contains(b.w) & (vm >> 7));
+    }
+  }
+  return cnt;
 }
 
-// Count, over in-edge records [kb, ke) taken 32 at a time with stride kstep,
-// the members of each suffix that `probe` accepts.  Suffixes are read as
-// aligned 16-byte quads (the padded layout keeps every quad in bounds); words
-// outside the suffix are masked.  All 32 lanes must call.
-template <typename Probe>
-__device__ __forceinline__ uint32_t walk_suffixes(const uint4 *__restrict__ adj4,
-                                                  const uint2 *__restrict__ edges, uint64_t kb,
-                                                  uint64_t ke, uint32_t kstep, int lane,
-                                                  Probe probe) {
+template <typename Set>
+__device__ __forceinline__ uint32_t walk_range(const uint4 *__restrict__ adj4,
+                                               const uint2 *__restrict__ edges, uint64_t kb,
+                                               uint64_t ke, int lane, const Set &set) {
   uint32_t cnt = 0;
-  for (uint64_t k = kb; k < ke; k += kstep) {
-    const uint64_t kk = k + lane;
-    uint32_t s = 0, e = 0, q0 = 0, nq = 0;
-    if (kk < ke) {
-      const uint2 r = edges[kk];
-      s = r.x;
-      e = r.x + r.y;
-      q0 = s >> 2;
-      nq = ((e + 3) >> 2) - q0;
-    }
-    const uint32_t incl = warp_inclusive_sum(nq, lane);
-    const uint32_t excl = incl - nq;
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    for (uint32_t pb = 0; pb < total; pb += 32) {
-      const uint32_t p = pb + lane;
-      const int o = warp_owner(incl, p);
-      const uint32_t ok = __shfl_sync(kFull, excl, o);
-      const uint32_t oq = __shfl_sync(kFull, q0, o);
-      const uint32_t os = __shfl_sync(kFull, s, o);
-      const uint32_t oe = __shfl_sync(kFull, e, o);
-      if (p < total) {
-        const uint32_t q = oq + (p - ok);
-        const uint4 x = adj4[q];
-        const uint32_t w = q * 4;
-        if (w >= os && w < oe) cnt += probe(x.x);
-        if (w + 1 >= os && w + 1 < oe) cnt += probe(x.y);
-        if (w + 2 >= os && w + 2 < oe) cnt += probe(x.z);
-        if (w + 3 >= os && w + 3 < oe) cnt += probe(x.w);
-      }
-    }
+  for (uint64_t k = kb; k < ke; k += 32) cnt += walk_chunk(adj4, edges, k, ke, lane, set);
+  return cnt;
+}
+
+// CTA tile: N+(v) does not fit a warp's set.  All warps share one set in the
+// whole shared buffer and claim 32-record chunks of the tile dynamically.
+template <int WARPS, typename Set>
+__device__ __forceinline__ uint32_t cta_walk(const uint4 *__restrict__ adj4,
+                                             const uint2 *__restrict__ edges, uint64_t kb,
+                                             uint64_t ke, uint32_t *chunk, int lane,
+                                             const Set &set) {
+  uint32_t cnt = 0;
+  while (true) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(chunk, 1u);
+    c = __shfl_sync(kFull, c, 0);
+    const uint64_t k = kb + (uint64_t)c * 32;
+    if (k >= ke) break;
+    cnt += walk_chunk(adj4, edges, k, ke < k + 32 ? ke : k + 32, lane, set);
   }
   return cnt;
 }
@@ -396,22 +393,26 @@ __device__ __forceinline__ uint32_t walk_suffixes(const uint4 *__restrict__ adj4
 template <int WARPS>
 __device__ uint32_t cta_tile(const GraphView &g, const uint2 *__restrict__ inedge,
                              const uint64_t *__restrict__ inptr, const Tile &t, uint32_t *smem,
-                             uint64_t *bar, uint32_t &phase, unsigned *err) {
+                             uint32_t *chunk, uint64_t *bar, uint32_t &phase, unsigned *err) {
   constexpr uint32_t S = WARPS * kWarpTableSlots;  // shared words
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   const uint32_t v = t.v0;
   const uint2 rv = g.row[v];
   const uint32_t d = rv.y;
   const uint32_t *av = g.adj + (uint64_t)rv.x * 4;
   const uint4 *adj4 = reinterpret_cast<const uint4 *>(g.adj);
   const uint64_t base = inptr[v];
-  const uint64_t kb = base + t.j0 + (uint64_t)warp * 32, ke = base + t.j1;
+  const uint64_t kb = base + t.j0, ke = base + t.j1;
+  const uint32_t lo = av[0], span = av[d - 1] - lo;
+  auto sync = [] { __syncthreads(); };
+  if (threadIdx.x == 0) *chunk = 0;
   uint32_t cnt = 0;
-  const uint32_t span = av[d - 1] - av[0];
-  if (span < S * 32u || 2 * d <= S) {
-    const MidSet st = build_set(av, d, smem, S, threadIdx.x, blockDim.x, [] { __syncthreads(); });
-    cnt = walk_suffixes(adj4, inedge, kb, ke, WARPS * 32, lane,
-                        [&](uint32_t x) { return st.contains(x); });
+  if (span <= bitmap_max_span(S)) {
+    const BitmapSet st = build_bitmap(av, d, lo, span, smem, threadIdx.x, blockDim.x, sync);
+    cnt = cta_walk<WARPS>(adj4, inedge, kb, ke, chunk, lane, st);
+  } else if (2 * d <= S) {
+    const BucketSet st = build_buckets(av, d, lo, span, smem, S, threadIdx.x, blockDim.x, sync);
+    cnt = cta_walk<WARPS>(adj4, inedge, kb, ke, chunk, lane, st);
   } else {
     // N+(v) staged whole (bulk copy) or sampled into shared memory; two-phase search
     if (d <= S) {
@@ -426,10 +427,8 @@ __device__ uint32_t cta_tile(const GraphView &g, const uint2 *__restrict__ inedg
       for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) smem[i] = av[(uint64_t)i * d / S];
       __syncthreads();
     }
-    const uint32_t lo = av[0], hi = av[d - 1];
-    cnt = walk_suffixes(adj4, inedge, kb, ke, WARPS * 32, lane, [&](uint32_t x) {
-      return (x >= lo && x <= hi) ? search_2phase(av, d, smem, S, x) : 0u;
-    });
+    const SearchSet st{av, smem, d, S, lo, span};
+    cnt = cta_walk<WARPS>(adj4, inedge, kb, ke, chunk, lane, st);
   }
   // the next tile rewrites shared memory, possibly through the async proxy
   fence_proxy_async_smem();
@@ -437,7 +436,7 @@ __device__ uint32_t cta_tile(const GraphView &g, const uint2 *__restrict__ inedg
   return cnt;
 }
 
-// One middle vertex v on one warp: set of N+(v) in the warp's slots, walk
+// One middle vertex v on one warp: a set of N+(v) in the warp's slots, walk
 // in-edges [j0, j1) of v.
 __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 *__restrict__ inedge,
                                                 const uint64_t *__restrict__ inptr, uint32_t v,
@@ -450,9 +449,17 @@ __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 
   const uint64_t kb = base + j0;
   if (d == 0 || kb >= ke) return 0;
   const uint32_t *av = g.adj + (uint64_t)rv.x * 4;
-  const MidSet st = build_set(av, d, tab, kWarpTableSlots, lane, 32, [] { __syncwarp(); });
-  const uint32_t c = walk_suffixes(reinterpret_cast<const uint4 *>(g.adj), inedge, kb, ke, 32, lane,
-                                   [&](uint32_t x) { return st.contains(x); });
+  const uint4 *adj4 = reinterpret_cast<const uint4 *>(g.adj);
+  const uint32_t lo = av[0], span = av[d - 1] - lo;
+  auto sync = [] { __syncwarp(); };
+  uint32_t c;
+  if (span <= kWarpBitmapSpan) {
+    const BitmapSet st = build_bitmap(av, d, lo, span, tab, lane, 32, sync);
+    c = walk_range(adj4, inedge, kb, ke, lane, st);
+  } else {
+    const BucketSet st = build_buckets(av, d, lo, span, tab, kWarpTableSlots, lane, 32, sync);
+    c = walk_range(adj4, inedge, kb, ke, lane, st);
+  }
   __syncwarp();
   return c;
 }
@@ -464,7 +471,7 @@ __global__ void __launch_bounds__(WARPS * 32, 2)
              TileRange rng, SchedState *sched, unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint64_t bar;
-  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_tile, s_chunk;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned long long cnt = 0;
 
@@ -475,7 +482,7 @@ __global__ void __launch_bounds__(WARPS * 32, 2)
   __syncthreads();
   uint32_t phase = 0;
 
-  // phase 1: CTA tiles (N+(v) larger than a warp's set)
+  // phase 1: CTA tiles (N+(v) does not fit a warp's set)
   while (true) {
     if (threadIdx.x == 0) s_tile = rng.cta_lo + atomicAdd(&sched->next_cta, 1u);
     __syncthreads();
@@ -483,7 +490,7 @@ __global__ void __launch_bounds__(WARPS * 32, 2)
     __syncthreads();
     if (t >= rng.cta_hi) break;
     const Tile tl = tiles[t];
-    cnt += cta_tile<WARPS>(g, inedge, inptr, tl, smem, &bar, phase, &sched->error);
+    cnt += cta_tile<WARPS>(g, inedge, inptr, tl, smem, &s_chunk, &bar, phase, &sched->error);
   }
 
   // phase 2: warp tiles, each warp on its own slots

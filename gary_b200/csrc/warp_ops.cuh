@@ -145,4 +145,99 @@ __device__ __forceinline__ uint32_t search_2phase(const uint32_t *list, uint32_t
   return 0;
 }
 
+// ---- shared-memory sets over a sorted list -------------------------------
+// All three answer contains(x) for x anywhere in [0, 2^32): values outside
+// [lo, lo + span] (including the UINT32_MAX padding) are rejected first.
+
+// Bitmap over [lo, lo + span]; branch-free probe.  The word after the
+// bitmap is a zero guard: an out-of-range value reads the guard (or the
+// never-set tail bits of the last word) and so tests 0.
+struct BitmapSet {
+  const uint32_t *mem;
+  uint32_t lo, guard;
+  __device__ __forceinline__ uint32_t contains(uint32_t x) const {
+    const uint32_t o = x - lo;
+    const uint32_t w = mem[min(o >> 5, guard)];
+    return __funnelshift_r(w, 0u, o) & 1u;  // w >> (o & 31)
+  }
+};
+
+// Bucketised open addressing: 4-slot buckets read with one 16-byte load.
+// Slots of a bucket fill in order, so a bucket with a free last slot ends
+// the probe sequence.
+struct BucketSet {
+  const uint4 *tab;
+  uint32_t lo, span, bmask;
+  int shift;
+  __device__ __forceinline__ uint32_t contains(uint32_t x) const {
+    if (x - lo > span) return 0;
+    uint32_t b = (x * kHashMul) >> shift;
+    while (true) {
+      const uint4 q = tab[b];
+      if (q.x == x || q.y == x || q.z == x || q.w == x) return 1;
+      if (q.w == kSentinel) return 0;
+      b = (b + 1) & bmask;
+    }
+  }
+};
+
+// Sorted copy (or samples) of the list in shared memory; two-phase search.
+struct SearchSet {
+  const uint32_t *list, *cache;
+  uint32_t len, S, lo, span;
+  __device__ __forceinline__ uint32_t contains(uint32_t x) const {
+    if (x - lo > span) return 0;
+    return search_2phase(list, len, cache, S, x);
+  }
+};
+
+// Builders: `nthreads` threads (a warp or the CTA) cooperate; `sync`
+// separates clear, fill and use.  They need span <= bitmap_max_span(words)
+// (bitmap) or d <= words / 2 (buckets) respectively.
+template <typename Sync>
+__device__ __forceinline__ BitmapSet build_bitmap(const uint32_t *__restrict__ av, uint32_t d,
+                                                  uint32_t lo, uint32_t span, uint32_t *mem,
+                                                  uint32_t tid, uint32_t nthreads, Sync sync) {
+  const uint32_t words = (span >> 5) + 2;  // bitmap + zero guard word
+  for (uint32_t i = tid; i < words; i += nthreads) mem[i] = 0;
+  sync();
+  for (uint32_t i = tid; i < d; i += nthreads) {
+    const uint32_t o = av[i] - lo;
+    atomicOr(&mem[o >> 5], 1u << (o & 31));
+  }
+  sync();
+  return BitmapSet{mem, lo, words - 1};
+}
+
+// Largest id span a bitmap of `words` shared words covers (guard included).
+__host__ __device__ constexpr uint32_t bitmap_max_span(uint32_t words) { return (words - 1) * 32u - 1u; }
+
+template <typename Sync>
+__device__ __forceinline__ BucketSet build_buckets(const uint32_t *__restrict__ av, uint32_t d,
+                                                   uint32_t lo, uint32_t span, uint32_t *mem,
+                                                   uint32_t words, uint32_t tid, uint32_t nthreads,
+                                                   Sync sync) {
+  // buckets = next power of two >= d, at most words / 4
+  int lb = d > 1 ? 32 - __clz(d - 1) : 0;
+  const int cap = 29 - __clz(words);  // log2(words / 4)
+  lb = lb < 3 ? 3 : (lb > cap ? cap : lb);
+  const uint32_t nb = 1u << lb;
+  for (uint32_t i = tid; i < 4 * nb; i += nthreads) mem[i] = kSentinel;
+  sync();
+  for (uint32_t i = tid; i < d; i += nthreads) {
+    const uint32_t x = av[i];
+    uint32_t b = (x * kHashMul) >> (32 - lb);
+    while (true) {
+      uint32_t *slot = mem + 4 * b;
+      if (atomicCAS(slot, kSentinel, x) == kSentinel) break;
+      if (atomicCAS(slot + 1, kSentinel, x) == kSentinel) break;
+      if (atomicCAS(slot + 2, kSentinel, x) == kSentinel) break;
+      if (atomicCAS(slot + 3, kSentinel, x) == kSentinel) break;
+      b = (b + 1) & (nb - 1);
+    }
+  }
+  sync();
+  return BucketSet{reinterpret_cast<const uint4 *>(mem), lo, span, nb - 1, 32 - lb};
+}
+
 }  // namespace gary
