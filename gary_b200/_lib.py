@@ -98,6 +98,8 @@ SIGNATURES = {
     "gary_count_async": (_INT, [_P, _INT, _INT, _P, _P]),
     "gary_count_shard_async": (_INT, [_P, _INT, _INT, _U32, _U32, _P, _P]),
     "gary_count_last_stats": (_INT, [_P, C.POINTER(CountStats)]),
+    "gary_tune": (_INT, [C.c_char_p, _U64]),
+    "gary_graph_drop_plans": (_INT, [_P]),
     "gary_csr_from_edges": (_INT, [_P, _P, _U64, _U32, _U32, _P, C.POINTER(_P)]),
     "gary_csr_info": (_INT, [_P, C.POINTER(_U32), C.POINTER(_U64)]),
     "gary_csr_device_ptrs": (_INT, [_P, C.POINTER(_P), C.POINTER(_P)]),

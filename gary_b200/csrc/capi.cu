@@ -8,6 +8,7 @@
 #include <exception>
 #include <mutex>
 #include <new>
+#include <string>
 
 #include "graph.cuh"
 #include "internal.cuh"
@@ -80,6 +81,9 @@ int guarded(const char *what, F &&f) {
 
 int plan_slot(int pattern, int sched) { return (pattern - 3) * 2 + sched; }
 
+PlanParams g_tuning;  // process-wide knobs of the counting plans (gary_tune)
+std::mutex g_tuning_mu;
+
 int count_async(gary_graph *g, int pattern, int sched, cudaStream_t s, unsigned long long *d_out,
                 uint32_t shard = 0, uint32_t nshards = 1) {
   GARY_CHECK_ARG(g != nullptr, "graph is NULL");
@@ -95,14 +99,44 @@ int count_async(gary_graph *g, int pattern, int sched, cudaStream_t s, unsigned 
     return GARY_ERR_UNSUPPORTED;
   }
   const int slot = plan_slot(pattern, sched);
-  if (!g->plans[slot]) GARY_TRY(build_k3_plan(g, PlanParams{}, s, &g->plans[slot]));
+  if (!g->plans[slot]) GARY_TRY(build_k3_plan(g, tuned_params(), s, &g->plans[slot]));
   return launch_k3(g, g->plans[slot], d_out, s, shard, nshards);
 }
 
 }  // namespace
+
+PlanParams tuned_params() {
+  std::lock_guard<std::mutex> lk(g_tuning_mu);
+  return g_tuning;
+}
+
 }  // namespace gary
 
 using gary::guarded;
+
+extern "C" int gary_tune(const char *key, uint64_t value) {
+  GARY_CHECK_ARG(key != nullptr, "key is NULL");
+  std::lock_guard<std::mutex> lk(gary::g_tuning_mu);
+  gary::PlanParams &p = gary::g_tuning;
+  const std::string k(key);
+  if (k == "warp_tile_cost" && value > 0) p.warp_tile_cost = value;
+  else if (k == "cta_tile_cost" && value > 0) p.cta_tile_cost = value;
+  else if (k == "vertex_overhead") p.vertex_overhead = value;
+  else if (k == "min_blocks" && (value == 2 || value == 3)) p.min_blocks = (uint32_t)value;
+  else if (k == "reset") p = gary::PlanParams{};
+  else {
+    gary::set_error("unknown tuning key '%s' or value %llu out of range", key,
+                    (unsigned long long)value);
+    return GARY_ERR_INVALID;
+  }
+  return GARY_OK;
+}
+
+extern "C" int gary_graph_drop_plans(gary_graph *g) {
+  GARY_CHECK_ARG(g != nullptr, "graph is NULL");
+  gary::free_plans(g);
+  return GARY_OK;
+}
 
 extern "C" const char *gary_last_error(void) { return gary::g_error; }
 

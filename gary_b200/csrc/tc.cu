@@ -21,6 +21,7 @@
 // tiles.
 #include <cub/cub.cuh>
 #include <thrust/binary_search.h>
+#include <thrust/copy.h>
 #include <thrust/execution_policy.h>
 #include <thrust/fill.h>
 #include <thrust/iterator/counting_iterator.h>
@@ -182,13 +183,25 @@ struct GroupTarget {
   __host__ __device__ uint64_t operator()(uint64_t g) const { return g * tw; }
 };
 
-__global__ void k_fill_group_tiles(const uint32_t *__restrict__ starts, uint64_t G, uint32_t n,
+struct IsLight {
+  const uint8_t *vclass;
+  __host__ __device__ bool operator()(uint32_t v) const { return vclass[v] == kClassLight; }
+};
+
+struct LightCost {
+  const uint64_t *cost;
+  __host__ __device__ uint64_t operator()(uint32_t v) const { return cost[v]; }
+};
+
+// Group tiles over the compacted light-vertex list: tile g covers list
+// positions [starts[g], starts[g+1]).
+__global__ void k_fill_group_tiles(const uint32_t *__restrict__ starts, uint64_t G, uint32_t L,
                                    Tile *__restrict__ tiles) {
   for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G;
        g += (uint64_t)gridDim.x * blockDim.x) {
     Tile t;
     t.v0 = starts[g];
-    t.v1 = g + 1 < G ? starts[g + 1] : n;
+    t.v1 = g + 1 < G ? starts[g + 1] : L;
     t.j0 = 0;
     t.j1 = kGroupTile;
     tiles[g] = t;
@@ -260,23 +273,20 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
   auto pol = thrust::cuda::par_nosync.on(s);
   GARY_TRY(build_in_index(g, s, plan->in));
   GARY_TRY(plan->vclass.alloc_persistent(n));
-  DevBuf<uint64_t> costL;
+  DevBuf<uint64_t> costV;  // cost of each light vertex, 0 for the others
   DevBuf<uint32_t> kW, kC;
-  GARY_TRY(costL.alloc((uint64_t)n + 1, s));
+  GARY_TRY(costV.alloc(n, s));
   GARY_TRY(kW.alloc((uint64_t)n + 1, s));
   GARY_TRY(kC.alloc((uint64_t)n + 1, s));
   k_classify<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, plan->in.work.p, plan->in.inptr.p, n, pp,
-                                              plan->vclass.p, costL.p, kW.p, kC.p);
+                                              plan->vclass.p, costV.p, kW.p, kC.p);
   GARY_CUDA(cudaGetLastError());
-  GARY_CUDA(cudaMemsetAsync(costL.p + n, 0, 8, s));
   GARY_CUDA(cudaMemsetAsync(kW.p + n, 0, 4, s));
   GARY_CUDA(cudaMemsetAsync(kC.p + n, 0, 4, s));
-  thrust::exclusive_scan(pol, costL.p, costL.p + n + 1, costL.p, 0ull);
+  const uint64_t totalL = thrust::reduce(pol, costV.p, costV.p + n, 0ull);
   thrust::exclusive_scan(pol, kW.p, kW.p + n + 1, kW.p, 0u);
   thrust::exclusive_scan(pol, kC.p, kC.p + n + 1, kC.p, 0u);
-  uint64_t totalL = 0;
   uint32_t nW = 0, nC = 0;
-  GARY_CUDA(cudaMemcpyAsync(&totalL, costL.p + n, 8, cudaMemcpyDeviceToHost, s));
   GARY_CUDA(cudaMemcpyAsync(&nW, kW.p + n, 4, cudaMemcpyDeviceToHost, s));
   GARY_CUDA(cudaMemcpyAsync(&nC, kC.p + n, 4, cudaMemcpyDeviceToHost, s));
   GARY_CUDA(cudaStreamSynchronize(s));
@@ -294,12 +304,23 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
                                                      plan->tiles.p + nC);
   GARY_CUDA(cudaGetLastError());
   if (G) {
+    // light vertices in id order, and the exclusive prefix of their costs
+    GARY_TRY(plan->light.alloc_persistent(n));
+    const uint32_t L = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                                  thrust::counting_iterator<uint32_t>(n),
+                                                  plan->light.p, IsLight{plan->vclass.p}) -
+                                  plan->light.p);
+    plan->n_light = L;
+    DevBuf<uint64_t> lc;
+    GARY_TRY(lc.alloc((uint64_t)L + 1, s));
+    auto costs = thrust::make_transform_iterator(plan->light.p, LightCost{costV.p});
+    thrust::exclusive_scan(pol, costs, costs + L, lc.p, 0ull);
     DevBuf<uint32_t> starts;
     GARY_TRY(starts.alloc(G, s));
     auto targets = thrust::make_transform_iterator(thrust::counting_iterator<uint64_t>(0),
                                                    GroupTarget{pp.warp_tile_cost});
-    thrust::lower_bound(pol, costL.p, costL.p + n, targets, targets + G, starts.p);
-    k_fill_group_tiles<<<grid_for(G), kThreads, 0, s>>>(starts.p, G, n, plan->tiles.p + nC + nW);
+    thrust::lower_bound(pol, lc.p, lc.p + L, targets, targets + G, starts.p);
+    k_fill_group_tiles<<<grid_for(G), kThreads, 0, s>>>(starts.p, G, L, plan->tiles.p + nC + nW);
     GARY_CUDA(cudaGetLastError());
   }
   GARY_TRY(plan->sched.alloc_persistent(1));
@@ -320,6 +341,21 @@ constexpr uint32_t kWarpBitmapSpan = bitmap_max_span(kWarpTableSlots);  // ids a
 // words at the end of adj keep every octet in bounds); the lanes walk the
 // concatenation of the chunk's octets, so short suffixes do not idle lanes.
 // Ids of an octet outside the suffix are masked.  All 32 lanes must call.
+// An octet of suffix ids in flight: its 8 words and the valid-word mask.
+struct Octet {
+  uint4 a, b;
+  uint32_t vm;
+};
+
+template <typename Set>
+__device__ __forceinline__ uint32_t probe_octet(const Octet &x, const Set &set) {
+  const uint32_t vm = x.vm;
+  return (set.contains(x.a.x) & vm) + (set.contains(x.a.y) & (vm >> 1)) +
+         (set.contains(x.a.z) & (vm >> 2)) + (set.contains(x.a.w) & (vm >> 3)) +
+         (set.contains(x.b.x) & (vm >> 4)) + (set.contains(x.b.y) & (vm >> 5)) +
+         (set.contains(x.b.z) & (vm >> 6)) + (set.contains(x.b.w) & (vm >> 7));
+}
+
 template <typename Set>
 __device__ __forceinline__ uint32_t walk_chunk(const uint4 *__restrict__ adj4,
                                                const uint2 *__restrict__ edges, uint64_t kb,
@@ -336,29 +372,40 @@ __device__ __forceinline__ uint32_t walk_chunk(const uint4 *__restrict__ adj4,
   const uint32_t incl = warp_inclusive_sum(no, lane);
   const uint32_t excl = incl - no;
   const uint32_t total = __shfl_sync(kFull, incl, 31);
-  uint32_t cnt = 0;
-  for (uint32_t pb = 0; pb < total; pb += 32) {
+  // Locate and load the octet of flattened position pb + lane (all lanes call).
+  auto fetch = [&](uint32_t pb) {
     const uint32_t p = pb + lane;
     const int o = warp_owner(incl, p);
     const uint32_t ox = __shfl_sync(kFull, excl, o);
     const uint32_t oo = __shfl_sync(kFull, o0, o);
     const uint32_t os = __shfl_sync(kFull, s, o);
     const uint32_t oe = __shfl_sync(kFull, e, o);
+    Octet x;
+    x.vm = 0;
     if (p < total) {
       const uint32_t oc = oo + (p - ox);
-      const uint4 a = adj4[2 * oc];
-      const uint4 b = adj4[2 * oc + 1];
+      x.a = adj4[2 * oc];
+      x.b = adj4[2 * oc + 1];
       const uint32_t w = oc * 8;
       // valid ids of this octet: words [max(w, os), min(w + 8, oe))
       const uint32_t skip = os > w ? os - w : 0u;
       const uint32_t keep = oe - w < 8u ? oe - w : 8u;
-      const uint32_t vm = ((1u << keep) - 1u) & ~((1u << skip) - 1u);
-      cnt += (set.contains(a.x) & vm) + (set.contains(a.y) & (vm >> 1)) +
-             (set.contains(a.z) & (vm >> 2)) + (set.contains(a.w) & (vm >> 3)) +
-             (set.contains(b.x) & (vm >> 4)) + (set.contains(b.y) & (vm >> 5)) +
-             (set.contains(b.z) & (vm >> 6)) + (set.contains(b.w) & (vm >> 7));
+      x.vm = ((1u << keep) - 1u) & ~((1u << skip) - 1u);
+    } else {
+      x.a = x.b = make_uint4(kSentinel, kSentinel, kSentinel, kSentinel);
     }
+    return x;
+  };
+  uint32_t cnt = 0;
+  if (total == 0) return 0;
+  // two batches in flight: the next octet loads while this one is probed
+  Octet cur = fetch(0);
+  for (uint32_t pb = 32; pb < total; pb += 32) {
+    const Octet nxt = fetch(pb);
+    cnt += probe_octet(cur, set);
+    cur = nxt;
   }
+  cnt += probe_octet(cur, set);
   return cnt;
 }
 
@@ -464,10 +511,10 @@ __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 
   return c;
 }
 
-template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 2)
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
     k_tc_mid(GraphView g, const uint2 *__restrict__ inedge, const uint64_t *__restrict__ inptr,
-             const uint8_t *__restrict__ vclass, const Tile *__restrict__ tiles, uint32_t n_cta,
+             const uint32_t *__restrict__ light, const Tile *__restrict__ tiles, uint32_t n_cta,
              TileRange rng, SchedState *sched, unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint64_t bar;
@@ -506,15 +553,12 @@ __global__ void __launch_bounds__(WARPS * 32, 2)
       cnt += warp_vertex(g, inedge, inptr, tl.v0, tl.j0, tl.j1, tab, lane);
       continue;
     }
-    for (uint32_t vb = tl.v0; vb < tl.v1; vb += 32) {
-      const uint32_t vv = vb + lane;
-      const bool light = vv < tl.v1 && vclass[vv] == kClassLight;
-      unsigned msk = __ballot_sync(kFull, light);
-      while (msk) {
-        const int k = __ffs(msk) - 1;
-        msk &= msk - 1;
-        cnt += warp_vertex(g, inedge, inptr, vb + k, 0, 0xFFFFFFFFu, tab, lane);
-      }
+    // a group of light vertices: list positions [v0, v1), 32 ids per load
+    for (uint32_t ib = tl.v0; ib < tl.v1; ib += 32) {
+      const uint32_t nb = min(32u, tl.v1 - ib);
+      const uint32_t myv = lane < nb ? light[ib + lane] : 0u;
+      for (uint32_t k = 0; k < nb; ++k)
+        cnt += warp_vertex(g, inedge, inptr, __shfl_sync(kFull, myv, k), 0, 0xFFFFFFFFu, tab, lane);
     }
   }
 
@@ -525,28 +569,28 @@ __global__ void __launch_bounds__(WARPS * 32, 2)
 
 }  // namespace
 
-int launch_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
-              uint32_t shard, uint32_t nshards) {
+template <int MINB>
+int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
+                   uint32_t shard, uint32_t nshards) {
   constexpr int WARPS = kTcWarps;
+  auto kern = k_tc_mid<WARPS, MINB>;
   const size_t smem = (size_t)WARPS * kWarpTableSlots * 4;
   static bool attr_done[64] = {false};
   const int dev = device_ordinal();
   if (dev < 64 && !attr_done[dev]) {
-    GARY_CUDA(cudaFuncSetAttribute(k_tc_mid<WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
+    GARY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_done[dev] = true;
   }
   int per_sm = 0;
-  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_mid<WARPS>, WARPS * 32, smem));
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem));
   if (per_sm < 1) per_sm = 1;
   const unsigned grid = (unsigned)(sm_count() * per_sm);
   const TileRange rng = shard_range(plan->n_cta, plan->n_warp, shard, nshards);
   GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
   GARY_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), s));
   GARY_CUDA(cudaEventRecord(g->ev0, s));
-  k_tc_mid<WARPS><<<grid, WARPS * 32, smem, s>>>(g->view(), plan->in.inedge.p, plan->in.inptr.p,
-                                                 plan->vclass.p, plan->tiles.p, plan->n_cta, rng,
-                                                 plan->sched.p, d_out);
+  kern<<<grid, WARPS * 32, smem, s>>>(g->view(), plan->in.inedge.p, plan->in.inptr.p, plan->light.p,
+                                      plan->tiles.p, plan->n_cta, rng, plan->sched.p, d_out);
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
@@ -554,6 +598,12 @@ int launch_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, c
   g->last.cta_tiles = rng.cta_hi - rng.cta_lo;
   g->last_timed = true;
   return GARY_OK;
+}
+
+int launch_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
+              uint32_t shard, uint32_t nshards) {
+  if (plan->params.min_blocks >= 3) return launch_k3_impl<3>(g, plan, d_out, s, shard, nshards);
+  return launch_k3_impl<2>(g, plan, d_out, s, shard, nshards);
 }
 
 }  // namespace gary

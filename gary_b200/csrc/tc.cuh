@@ -17,7 +17,8 @@ enum : uint8_t { kClassNone = 0, kClassLight = 1, kClassSplit = 2, kClassCta = 3
 enum : uint32_t { kVarHash = 0, kVarSearch = 1, kVarMerge = 2, kVarBitmap = 3 };
 
 // A unit of scheduled work over middle vertices v.
-//   j1 == kGroupTile : every light vertex v in [v0, v1), all its in-edges
+//   j1 == kGroupTile : light vertices light[v0 .. v1) (the plan's compacted
+//                      list of light vertices), all their in-edges
 //   otherwise        : vertex v0 only, in-edges [j0, j1) of its in-list
 struct Tile {
   uint32_t v0, v1, j0, j1;
@@ -28,7 +29,11 @@ struct PlanParams {
   uint64_t warp_tile_cost = 1u << 15;       // target probes per warp tile
   uint64_t cta_tile_cost = 1u << 20;        // target probes per CTA tile
   uint64_t vertex_overhead = 64;            // fixed cost of a middle vertex
+  uint32_t min_blocks = 2;                  // resident CTAs per SM the kernel is built for
 };
+
+// Process-wide tuning overrides (0 = keep the default), set by gary_tune().
+PlanParams tuned_params();
 
 // Contiguous tile ranges of one shard (multi-GPU: every rank holds the whole
 // graph and counts its own ranges; the partial counts are summed).
@@ -71,6 +76,8 @@ struct gary_count_plan {
   gary::PlanParams params;
   gary::InIndex in;
   gary::DevBuf<uint8_t> vclass;
+  gary::DevBuf<uint32_t> light;  // light vertices (group tiles index this list)
+  uint32_t n_light = 0;
   gary::DevBuf<gary::Tile> tiles;
   uint32_t n_cta = 0;
   uint32_t n_warp = 0;

@@ -158,6 +158,19 @@ typedef struct gary_count_stats {
 } gary_count_stats;
 int gary_count_last_stats(gary_graph *g, gary_count_stats *out);
 
+/* ---- tuning (the autotuner's knobs) -------------------------------------
+ * Process-wide parameters of the counting plans, applied to plans built after
+ * the call (gary_graph_drop_plans discards a graph's cached plans):
+ *   "warp_tile_cost"  target probes per warp tile        (default 2^15)
+ *   "cta_tile_cost"   target probes per CTA tile         (default 2^20)
+ *   "vertex_overhead" fixed cost charged per vertex      (default 64)
+ *   "min_blocks"      resident CTAs per SM, 2 or 3       (default 2)
+ *   "reset"           restore every default
+ * No reference counterpart: the reference fixes its launch shape in each test
+ * (test/TriQueryTest.cu:98-99, 116-117). */
+int gary_tune(const char *key, uint64_t value);
+int gary_graph_drop_plans(gary_graph *g);
+
 /* ---- symmetric CSR construction on the device ------------------------- *
  * Dedup, drop self loops, symmetrise and sort an undirected edge list into a
  * CSR (the reference does this on the host: src/Graph.cpp:19-32, 63-91). */
