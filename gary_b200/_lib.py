@@ -98,6 +98,7 @@ SIGNATURES = {
     "gary_count_async": (_INT, [_P, _INT, _INT, _P, _P]),
     "gary_count_shard_async": (_INT, [_P, _INT, _INT, _U32, _U32, _P, _P]),
     "gary_count_last_stats": (_INT, [_P, C.POINTER(CountStats)]),
+    "gary_count_triangles_noalloc": (_INT, [_P, _P, _P, _U32, _P, _P]),
     "gary_tune": (_INT, [C.c_char_p, _U64]),
     "gary_graph_drop_plans": (_INT, [_P]),
     "gary_csr_from_edges": (_INT, [_P, _P, _U64, _U32, _U32, _P, C.POINTER(_P)]),

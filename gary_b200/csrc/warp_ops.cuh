@@ -203,7 +203,7 @@ __device__ __forceinline__ BitmapSet build_bitmap(const uint32_t *__restrict__ a
   sync();
   for (uint32_t i = tid; i < d; i += nthreads) {
     const uint32_t o = av[i] - lo;
-    atomicOr(&mem[o >> 5], 1u << (o & 31));
+    if (o <= span) atomicOr(&mem[o >> 5], 1u << (o & 31));  // always true for a sorted list
   }
   sync();
   return BitmapSet{mem, lo, words - 1};

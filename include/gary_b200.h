@@ -158,6 +158,23 @@ typedef struct gary_count_stats {
 } gary_count_stats;
 int gary_count_last_stats(gary_graph *g, gary_count_stats *out);
 
+/* ---- triangle count without device allocation --------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (all device memory owned by a host framework's pool, or a fixed memory
+ * budget): the caller passes an oriented CSR already on the device, in the
+ * DeviceCSR layout (indptr[v] = first entry of v, deg[v] = its length; every
+ * undirected edge stored once, any acyclic orientation, lists sorted), and a
+ * device word for the result.  The library allocates nothing: its only
+ * scratch is a 128 KiB file-scope device array that every GPU loading the
+ * library holds until exit, and n may be at most 33,550,336 vertices (larger
+ * n returns GARY_ERR_INVALID).  The first call on a device looks up that
+ * array's device address and should come before any stream capture.  All
+ * calls share the array, so calls that overlap on the GPU race; each call
+ * clears it before use.  Asynchronous on `stream`. */
+int gary_count_triangles_noalloc(const uint64_t *d_indptr, const uint32_t *d_colidx,
+                                 const uint32_t *d_deg, uint32_t n, void *stream,
+                                 uint64_t *d_out);
+
 /* ---- tuning (the autotuner's knobs) -------------------------------------
  * Process-wide parameters of the counting plans, applied to plans built after
  * the call (gary_graph_drop_plans discards a graph's cached plans):
