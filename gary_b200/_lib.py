@@ -33,6 +33,11 @@ GARY_PATTERN_4CLIQUE = 5
 GARY_SCHED_PLAIN = 0
 GARY_SCHED_LEARNED = 1
 
+GARY_ISECT_AUTO = 0
+GARY_ISECT_MERGE = 1
+GARY_ISECT_SEARCH = 2
+GARY_ISECT_BITMAP = 3
+
 
 class GraphInfo(C.Structure):
     _fields_ = [
@@ -100,6 +105,12 @@ SIGNATURES = {
     "gary_count_last_stats": (_INT, [_P, C.POINTER(CountStats)]),
     "gary_count_triangles_noalloc": (_INT, [_P, _P, _P, _U32, _P, _P]),
     "gary_tune": (_INT, [C.c_char_p, _U64]),
+    "gary_intersect_batch": (_INT, [_U64, _P, _P, _P, _P, _P, _P, _INT, _P, _P, _P, _P, _P, _P]),
+    "gary_search_batch": (_INT, [_P, _U64, _P, _U64, _U32, _P, _P, _P]),
+    "gary_zipf_table": (_INT, [_U32, C.c_double, _P]),
+    "gary_gen_pair_host": (_INT, [_U64, _U64, _U32, _P, C.c_double, _U64, _P, _P, _P, _P]),
+    "gary_gen_pairs_lengths": (_INT, [_U64, _U64, _U64, _U32, _P, _P, _P, _P, _P, _P]),
+    "gary_gen_pairs_values": (_INT, [_U64, _U64, _U64, _U32, _P, C.c_double, _U64, _P, _P, _P, _P, _P, _P, _P]),
     "gary_graph_drop_plans": (_INT, [_P]),
     "gary_csr_from_edges": (_INT, [_P, _P, _U64, _U32, _U32, _P, C.POINTER(_P)]),
     "gary_csr_info": (_INT, [_P, C.POINTER(_U32), C.POINTER(_U64)]),

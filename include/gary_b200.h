@@ -188,6 +188,54 @@ int gary_count_triangles_noalloc(const uint64_t *d_indptr, const uint32_t *d_col
 int gary_tune(const char *key, uint64_t value);
 int gary_graph_drop_plans(gary_graph *g);
 
+/* ---- batched set operations: the include/ops layer ---------------------
+ * Lists are sorted ascending, values < UINT32_MAX. */
+#define GARY_ISECT_AUTO 0   /* SEARCH when the longer list is much longer, else MERGE */
+#define GARY_ISECT_MERGE 1  /* warp merge path over 32-wide windows (ballot / shuffle) */
+#define GARY_ISECT_SEARCH 2 /* two-phase search: 256 shared samples, then HBM */
+#define GARY_ISECT_BITMAP 3 /* shared bitmap of the longer list over 32K-value windows */
+
+/* |A_i & B_i| for npairs pairs; A_i = d_a[d_a_off[i] .. + d_a_len[i]), B_i likewise.
+ * Replaces intersectBinarySearch / intersect (include/ops/Intersection.cuh:18-199)
+ * and intersect_bs_cache (Intersection.cuh:240-300), which intersect one pair
+ * per warp inside a caller's kernel.  d_counts[i] (optional) receives each
+ * count, *d_total (optional) their sum.  With d_out_off set, A_i & B_i is
+ * also written, sorted, to d_out + d_out_off[i] (capacity min(|A_i|,|B_i|)).
+ * d_queue is one device word of scheduler state owned by the caller. */
+int gary_intersect_batch(uint64_t npairs, const uint64_t *d_a_off, const uint32_t *d_a_len,
+                         const uint32_t *d_a, const uint64_t *d_b_off, const uint32_t *d_b_len,
+                         const uint32_t *d_b, int variant, uint64_t *d_counts,
+                         const uint64_t *d_out_off, uint32_t *d_out, uint64_t *d_total,
+                         uint64_t *d_queue, void *stream);
+
+/* Search nkeys keys in one sorted list (duplicates allowed).  cache_entries = 0:
+ * binary_search (include/ops/Search.cuh:48-61); otherwise the two-phase search
+ * of Search.cuh:93-138 with that many samples cached per CTA (the reference
+ * uses 32; up to 8192).  d_found[i] = 1 when keys[i] is present (optional);
+ * *d_count = number present (optional). */
+int gary_search_batch(const uint32_t *d_list, uint64_t len, const uint32_t *d_keys, uint64_t nkeys,
+                      uint32_t cache_entries, uint8_t *d_found, uint64_t *d_count, void *stream);
+
+/* Set-intersection workload generator (seeded, counter-based; identical on
+ * host and device).  gary_zipf_table fills cdf[nmax] with uint64 thresholds
+ * of Zipf(s) on [1, nmax] (inverse-CDF sampling; the reference draws Zipf by
+ * rejection-inversion, common/Zipf.h:34-172).  Lists of pair i have
+ * Zipf lengths and one uniform value per bucket of [0, range); a fraction
+ * `overlap` of the shorter list is planted from the longer one.  Device
+ * generation is two calls: lengths (and 16-byte-padded quad counts, whose
+ * exclusive scan times 4 gives the offsets), then values. */
+int gary_zipf_table(uint32_t nmax, double s, uint64_t *cdf);
+int gary_gen_pair_host(uint64_t seed, uint64_t pair, uint32_t nmax, const uint64_t *cdf,
+                       double overlap, uint64_t range, uint32_t *a, uint32_t *la, uint32_t *b,
+                       uint32_t *lb);
+int gary_gen_pairs_lengths(uint64_t seed, uint64_t first, uint64_t npairs, uint32_t nmax,
+                           const uint64_t *d_cdf, uint32_t *d_la, uint32_t *d_lb, uint64_t *d_qa,
+                           uint64_t *d_qb, void *stream);
+int gary_gen_pairs_values(uint64_t seed, uint64_t first, uint64_t npairs, uint32_t nmax,
+                          const uint64_t *d_cdf, double overlap, uint64_t range,
+                          const uint32_t *d_la, const uint32_t *d_lb, const uint64_t *d_a_off,
+                          const uint64_t *d_b_off, uint32_t *d_a, uint32_t *d_b, void *stream);
+
 /* ---- symmetric CSR construction on the device ------------------------- *
  * Dedup, drop self loops, symmetrise and sort an undirected edge list into a
  * CSR (the reference does this on the host: src/Graph.cpp:19-32, 63-91). */

@@ -107,7 +107,9 @@ def main():
                                       (2, 100, 500, 0, 200, True),
                                       (3, 31, 64, 0, 64, False),
                                       (4, 1, 8, 0, 4, True),
-                                      (5, 70000, 4096, 1 << 26, 1 << 30, True)):
+                                      (5, 70000, 4096, 1 << 26, 1 << 30, True),
+                                      (6, 4096, 4096, 0, 8192, True),
+                                      (7, 100000, 8192, 0, 150000, False)):
         lst, keys = search_case(seed, nl, nk, lo, hi, sk)
         f1, f2 = O.ref_search(lst, keys)
         out["search"].append({
