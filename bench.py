@@ -51,6 +51,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU sample time")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference GPU kernel")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", choices=["tc", "setops"], default="tc",
+                    help="tc: the headline triangle count; setops: the set-intersection microbench")
+    ap.add_argument("--pairs-log2", type=int, default=24, help="setops: total pairs = 2^k")
+    ap.add_argument("--batch-log2", type=int, default=20, help="setops: pairs per generated batch")
+    ap.add_argument("--overlaps", default="0,0.1,0.25,0.5", help="setops: planted overlap fractions")
     return ap.parse_args()
 
 
@@ -404,9 +409,72 @@ def run_ours(args, dist):
     return 0
 
 
+def run_setops(args, dist):
+    """Set-intersection microbench: 2^pairs_log2 pairs of sorted uint32 lists,
+    Zipf(1.2) lengths on [1, 65536], values in [0, 2^26), per planted overlap;
+    merge / two-phase search / bitmap, count-only and materialised.  Pairs are
+    generated on the device in batches (not timed); each variant's kernel is
+    timed with CUDA events on every batch."""
+    import numpy as np
+    import torch
+
+    from gary_b200 import setops as so
+
+    torch.cuda.set_device(dist.local)
+    cdf = so.zipf_table(65536, 1.2)
+    total_pairs = 1 << args.pairs_log2
+    bsz = min(1 << args.batch_log2, total_pairs)
+    overlaps = [float(x) for x in args.overlaps.split(",")]
+    variants = ["merge", "search", "bitmap", "auto"]
+    res = {}
+    stream = torch.cuda.Stream()
+    for ov in overlaps:
+        acc = {(v, m): [0.0, 0] for v in variants for m in (False, True)}
+        bytes_in = 0
+        out_elems = 0
+        for first in range(0, total_pairs, bsz):
+            with torch.cuda.stream(stream):
+                batch = so.PairBatch.generate(args.seed, first, bsz, cdf, ov, stream=stream)
+            stream.synchronize()
+            bytes_in += batch.input_bytes()
+            for v in variants:
+                for mat in (False, True):
+                    with torch.cuda.stream(stream):
+                        so.intersect(batch, so.VARIANTS[v], mat, stream=stream)  # warm
+                        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                        r = so.intersect(batch, so.VARIANTS[v], mat, stream=stream)
+                        e1.record(stream)
+                    stream.synchronize()
+                    acc[(v, mat)][0] += e0.elapsed_time(e1)
+                    acc[(v, mat)][1] = acc[(v, mat)][1] + int(r[1].item())
+            del batch
+        for (v, mat), (ms, hits) in acc.items():
+            if v == "merge" and not mat:
+                out_elems = hits
+            b = bytes_in + (4 * hits if mat else 0)
+            res[f"ov{ov}:{v}:{'mat' if mat else 'count'}"] = {
+                "pairs_per_s": total_pairs / (ms / 1e3), "ms": ms, "GB_per_s": b / (ms / 1e3) / 1e9,
+                "intersection_total": hits}
+        # every variant agrees on the total
+        totals = {k: r["intersection_total"] for k, r in res.items() if k.startswith(f"ov{ov}:")}
+        assert len(set(totals.values())) == 1, totals
+    best = max((r["pairs_per_s"], k) for k, r in res.items() if k.endswith(":count"))
+    line = {"metric": "set-intersection pairs/sec (2^24 Zipf(1.2) pairs)", "value": best[0], "unit": "pairs/s",
+            "best": best[1], "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"set-intersection microbench, 2^{args.pairs_log2} pairs per overlap, "
+                                   f"Zipf(1.2) lengths on [1, 65536], values in [0, 2^26)",
+                       "batch_pairs": bsz, "overlaps": overlaps, "seed": args.seed},
+            "variants": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     dist = Dist()
+    if args.workload == "setops":
+        return run_setops(args, dist)
     if args.impl == "reference":
         return run_reference(args, dist)
     return run_ours(args, dist)
