@@ -12,6 +12,7 @@
 
 #include "graph.cuh"
 #include "internal.cuh"
+#include "patterns.cuh"
 #include "tc.cuh"
 
 namespace gary {
@@ -58,6 +59,9 @@ void free_plans(gary_graph *g) {
     delete p;
     p = nullptr;
   }
+  delete g->k4_plan;
+  delete g->c4_plan;
+  g->k4_plan = g->c4_plan = nullptr;
 }
 
 namespace {
@@ -94,8 +98,21 @@ int count_async(gary_graph *g, int pattern, int sched, cudaStream_t s, unsigned 
   GARY_CHECK_ARG(sched == GARY_SCHED_PLAIN || sched == GARY_SCHED_LEARNED, "unknown scheduler %d",
                  sched);
   GARY_CHECK_ARG(nshards >= 1 && shard < nshards, "shard %u of %u is out of range", shard, nshards);
-  if (pattern != GARY_PATTERN_TRIANGLE || sched != GARY_SCHED_PLAIN) {
-    set_error("pattern %d with scheduler %d is not available in this build", pattern, sched);
+  if (pattern == GARY_PATTERN_4CLIQUE) {
+    if (g->dag.max_len > kK4MaxOutDegree) {
+      set_error("4-clique counting supports out-degree <= %u (graph has %u)", kK4MaxOutDegree,
+                g->dag.max_len);
+      return GARY_ERR_UNSUPPORTED;
+    }
+    if (!g->k4_plan) GARY_TRY(build_k4_plan(g, s, &g->k4_plan));
+    return launch_k4(g, g->k4_plan, d_out, s, shard, nshards);
+  }
+  if (pattern == GARY_PATTERN_4CYCLE) {
+    if (!g->c4_plan) GARY_TRY(build_c4_plan(g, s, &g->c4_plan));
+    return launch_c4(g, g->c4_plan, d_out, s, shard, nshards);
+  }
+  if (sched != GARY_SCHED_PLAIN) {
+    set_error("scheduler %d is not available in this build", sched);
     return GARY_ERR_UNSUPPORTED;
   }
   const int slot = plan_slot(pattern, sched);
@@ -227,9 +244,12 @@ extern "C" int gary_count(gary_graph *g, int pattern, int sched, void *stream, u
     GARY_TRY(gary::count_async(g, pattern, sched, s, g->result.p));
     unsigned long long h = 0;
     gary::SchedState st{};
-    gary_count_plan *plan = g->plans[gary::plan_slot(pattern, sched)];
+    const gary::SchedState *dst = nullptr;
+    if (pattern == GARY_PATTERN_TRIANGLE) dst = g->plans[gary::plan_slot(pattern, sched)]->sched.p;
+    else if (pattern == GARY_PATTERN_4CLIQUE) dst = g->k4_plan->sched.p;
+    else dst = g->c4_plan->sched.p;
     GARY_CUDA(cudaMemcpyAsync(&h, g->result.p, sizeof(h), cudaMemcpyDeviceToHost, s));
-    GARY_CUDA(cudaMemcpyAsync(&st, plan->sched.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaMemcpyAsync(&st, dst, sizeof(st), cudaMemcpyDeviceToHost, s));
     GARY_CUDA(cudaStreamSynchronize(s));
     if (st.error) {
       gary::set_error("a bounded device wait expired (error word 0x%x)", st.error);

@@ -602,6 +602,54 @@ int build_coo(PaddedCSR &c, cudaStream_t s) {
   return GARY_OK;
 }
 
+namespace {
+// both directions of every oriented edge, from the padded DAG
+__global__ void k_sym_keys(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
+                           const uint32_t *__restrict__ rowid, uint64_t words, int lg,
+                           uint64_t *__restrict__ keys) {
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = rowid[w];
+    const uint2 r = row[u];
+    const uint64_t pos = w - (uint64_t)r.x * 4;
+    if (pos < r.y) {
+      const uint64_t v = adj[w];
+      keys[2 * w] = ((uint64_t)u << lg) | v;
+      keys[2 * w + 1] = (v << lg) | u;
+    } else {
+      keys[2 * w] = keys[2 * w + 1] = ~0ull;
+    }
+  }
+}
+}  // namespace
+
+// Symmetric lists in rank ids (for 4-cycle counting), built once on demand.
+int build_symmetric(gary_graph *g, cudaStream_t s) {
+  if (g->sym.row.p) return GARY_OK;
+  auto pol = thrust::cuda::par_nosync.on(s);
+  const uint32_t n = g->n;
+  const int lg = bits_for(n);
+  const uint64_t W = g->dag.words;
+  DevBuf<uint64_t> keys;
+  uint64_t m2 = 0;
+  {
+    DevBuf<uint32_t> rowid;
+    GARY_TRY(padded_rowid(g->dag, rowid, s));
+    GARY_TRY(keys.alloc(std::max<uint64_t>(2 * W, 1), s));
+    if (W) k_sym_keys<<<grid_for(W), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, rowid.p, W, lg, keys.p);
+    GARY_CUDA(cudaGetLastError());
+    m2 = thrust::remove(pol, keys.p, keys.p + 2 * W, ~0ull) - keys.p;
+  }
+  {
+    DevBuf<uint64_t> alt;
+    GARY_TRY(alt.alloc(std::max<uint64_t>(m2, 1), s));
+    if (m2) GARY_TRY(radix_sort_keys(keys, alt, m2, 2 * lg, s));
+  }
+  GARY_TRY(padded_from_keys(keys, m2, n, lg, g->sym, s));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  return GARY_OK;
+}
+
 int download(gary_graph *g, uint64_t *ptr, uint32_t *idx, uint32_t *perm, cudaStream_t s) {
   PaddedCSR &c = g->user_view();
   GARY_TRY(build_coo(c, s));

@@ -23,6 +23,7 @@
 struct gary_count_plan;  // tc.cu: cached tile lists per (pattern, sched)
 
 namespace gary {
+struct PatternPlan;  // patterns.cu: 4-clique / 4-cycle plans
 struct PaddedCSR {
   uint32_t n = 0;
   uint64_t m = 0;      // stored ids
@@ -60,6 +61,8 @@ struct gary_graph {
   gary::PaddedCSR sym;
 
   gary_count_plan *plans[8] = {nullptr};
+  gary::PatternPlan *k4_plan = nullptr;
+  gary::PatternPlan *c4_plan = nullptr;
   gary::DevBuf<unsigned long long> result;  // device word for gary_count
   gary_count_stats last{};
   bool last_timed = false;  // ev0/ev1 bracket the last counting kernel
@@ -76,4 +79,6 @@ namespace gary {
 void free_plans(gary_graph *g);
 // rowid[w] = row owning padded word w of `c`
 int padded_rowid(const PaddedCSR &c, DevBuf<uint32_t> &rowid, cudaStream_t s);
+// g->sym: both directions of every edge, rank ids, sorted, padded
+int build_symmetric(gary_graph *g, cudaStream_t s);
 }  // namespace gary

@@ -1,0 +1,585 @@
+// 4-clique and 4-cycle counting.  The reference declares a second pattern
+// kernel (rectCountHom, include/kernels/GraphQueryHom.cuh:48) but never
+// defines it; these kernels are new, pinned by the CPU oracle and closed-form
+// known answers.
+//
+// 4-cliques (degree-ranked DAG, every list in orientation order):
+//   K4 = sum over u, over v in N+(u), over w in S = N+(u) & N+(v) of |S & N+(w)|
+// counts each clique u < v < w < x once.  One warp (or CTA) holds N+(u) as a
+// shared hash set whose slots carry one membership bit per warp.  For each
+// middle vertex v it streams N+(v) three times: (A) mark the members of S,
+// (B) for the marked w, walk N+(w) (flattened across the w's of a 32-wide
+// step) counting marked hits, (C) clear the marks.  No buffer for S is
+// needed, so S can be as long as N+(u).
+//
+// 4-cycles (symmetric ranked lists): each cycle is counted once at its
+// highest-ranked vertex u, with w the opposite vertex:
+//   C4 = sum over u, over w < u of C(c(u,w), 2),
+//   c(u,w) = |{v < u : v adjacent to u and to w}|.
+// The wedges u-v-w (v, w < u) are walked and c(u,w) is accumulated in a
+// counter map; adding the counter's old value at every increment sums
+// C(c, 2) directly.  Warps use a shared-memory map; vertices with more
+// wedges than it holds use a per-CTA dense counter array in HBM that is
+// reset by a second walk.
+#include <thrust/binary_search.h>
+#include <thrust/copy.h>
+#include <thrust/execution_policy.h>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
+#include <thrust/reduce.h>
+#include <thrust/scan.h>
+
+#include <algorithm>
+#include <memory>
+
+#include "graph.cuh"
+#include "patterns.cuh"
+#include "warp_ops.cuh"
+
+namespace gary {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPWarps = 8;
+constexpr uint32_t kPSlots = 1024;  // per-warp hash slots
+constexpr uint32_t kCtaSlots = 8192;
+
+inline unsigned grid_for(uint64_t items) {
+  uint64_t b = (items + kThreads - 1) / kThreads;
+  uint64_t cap = (uint64_t)sm_count() * 16;
+  return (unsigned)std::max<uint64_t>(std::min(b, cap), 1);
+}
+
+__host__ __device__ __forceinline__ uint64_t min64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+// ---- tagged hash set of N+(u) --------------------------------------------
+struct TagSet {
+  uint32_t *keys, *tags;
+  uint32_t mask;
+  int shift;
+  __device__ __forceinline__ int find(uint32_t x) const {
+    uint32_t h = (x * kHashMul) >> shift;
+    while (true) {
+      const uint32_t k = keys[h];
+      if (k == x) return (int)h;
+      if (k == kSentinel) return -1;
+      h = (h + 1) & mask;
+    }
+  }
+};
+
+template <typename Sync>
+__device__ __forceinline__ TagSet build_tagset(const uint32_t *__restrict__ keys_in, uint32_t lo,
+                                               uint32_t hi, uint32_t *keys, uint32_t *tags,
+                                               uint32_t slots, uint32_t tid, uint32_t nthreads,
+                                               Sync sync) {
+  const uint32_t d = hi - lo;
+  int l = d > 1 ? 32 - __clz(2 * d - 1) : 1;
+  const int cap = 31 - __clz(slots);
+  l = l < 5 ? 5 : (l > cap ? cap : l);
+  for (uint32_t i = tid; i < (1u << l); i += nthreads) {
+    keys[i] = kSentinel;
+    tags[i] = 0;
+  }
+  sync();
+  hash_insert_range(keys, l, keys_in, lo, hi, tid, nthreads);
+  sync();
+  return TagSet{keys, tags, (1u << l) - 1, 32 - l};
+}
+
+// K4 work for one (u, v): |S & N+(w)| summed over w in S, S = set & N+(v).
+__device__ uint32_t k4_middle(const GraphView &g, const TagSet &ts, uint32_t v, uint32_t bit,
+                              int lane) {
+  const uint2 rv = g.row[v];
+  const uint32_t dv = rv.y;
+  if (dv < 2) return 0;
+  const uint32_t *av = g.adj + (uint64_t)rv.x * 4;
+  // (A) mark S
+  for (uint32_t k = lane; k < dv; k += 32) {
+    const int sl = ts.find(av[k]);
+    if (sl >= 0) atomicOr(&ts.tags[sl], bit);
+  }
+  __syncwarp();
+  // (B) for every w in S, count marked members of N+(w)
+  uint32_t cnt = 0;
+  for (uint32_t k0 = 0; k0 < dv; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    uint32_t len = 0, base = 0;
+    if (k < dv) {
+      const uint32_t w = av[k];
+      if (ts.find(w) >= 0) {
+        const uint2 rw = g.row[w];
+        len = rw.y;
+        base = rw.x;
+      }
+    }
+    const uint32_t incl = warp_inclusive_sum(len, lane);
+    const uint32_t excl = incl - len;
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    for (uint32_t pb = 0; pb < total; pb += 32) {
+      const uint32_t p = pb + lane;
+      const int o = warp_owner(incl, p);
+      const uint32_t ox = __shfl_sync(kFull, excl, o);
+      const uint32_t ob = __shfl_sync(kFull, base, o);
+      if (p < total) {
+        const int sl = ts.find(g.adj[(uint64_t)ob * 4 + (p - ox)]);
+        cnt += (sl >= 0 && (ts.tags[sl] & bit)) ? 1u : 0u;
+      }
+    }
+  }
+  __syncwarp();
+  // (C) clear the marks
+  for (uint32_t k = lane; k < dv; k += 32) {
+    const int sl = ts.find(av[k]);
+    if (sl >= 0) atomicAnd(&ts.tags[sl], ~bit);
+  }
+  __syncwarp();
+  return cnt;
+}
+
+__global__ void __launch_bounds__(kPWarps * 32)
+    k_k4(GraphView g, const Tile *__restrict__ tiles, const uint32_t *__restrict__ light,
+         uint32_t n_cta, TileRange rng, SchedState *sched, unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  __shared__ uint32_t s_tile, s_next;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long cnt = 0;
+  // phase 1: CTA tiles (d+(u) beyond a warp table); one shared table, a
+  // membership bit per warp, middle vertices claimed dynamically
+  while (true) {
+    if (threadIdx.x == 0) {
+      s_tile = rng.cta_lo + atomicAdd(&sched->next_cta, 1u);
+      s_next = 0;
+    }
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= rng.cta_hi) break;
+    const Tile tl = tiles[t];
+    const uint32_t u = tl.v0;
+    const uint2 ru = g.row[u];
+    const uint32_t *au = g.adj + (uint64_t)ru.x * 4;
+    const TagSet ts = build_tagset(au, tl.j0 + 1, ru.y, sm, sm + kCtaSlots, kCtaSlots, threadIdx.x,
+                                   blockDim.x, [] { __syncthreads(); });
+    const uint32_t j1 = min(tl.j1, ru.y - 2);
+    while (true) {
+      uint32_t j = 0;
+      if (lane == 0) j = tl.j0 + atomicAdd(&s_next, 1u);
+      j = __shfl_sync(kFull, j, 0);
+      if (j >= j1) break;
+      cnt += k4_middle(g, ts, au[j], 1u << warp, lane);
+    }
+    __syncthreads();
+  }
+  // phase 2: warp tiles
+  uint32_t *keys = sm + warp * 2 * kPSlots, *tags = keys + kPSlots;
+  const Tile *wt = tiles + n_cta;
+  auto do_u = [&](uint32_t u, uint32_t j0, uint32_t j1) {
+    const uint2 ru = g.row[u];
+    if (ru.y < 3) return;
+    j1 = min(j1, ru.y - 2);
+    if (j0 >= j1) return;
+    const uint32_t *au = g.adj + (uint64_t)ru.x * 4;
+    const TagSet ts = build_tagset(au, j0 + 1, ru.y, keys, tags, kPSlots, lane, 32,
+                                   [] { __syncwarp(); });
+    for (uint32_t j = j0; j < j1; ++j) cnt += k4_middle(g, ts, au[j], 1u, lane);
+    __syncwarp();
+  };
+  while (true) {
+    uint32_t t = 0;
+    if (lane == 0) t = rng.warp_lo + atomicAdd(&sched->next_warp, 1u);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= rng.warp_hi) break;
+    const Tile tl = wt[t];
+    if (tl.j1 != kGroupTile) {
+      do_u(tl.v0, tl.j0, tl.j1);
+      continue;
+    }
+    for (uint32_t ib = tl.v0; ib < tl.v1; ib += 32) {
+      const uint32_t nb = min(32u, tl.v1 - ib);
+      const uint32_t myu = lane < nb ? light[ib + lane] : 0u;
+      for (uint32_t k = 0; k < nb; ++k) do_u(__shfl_sync(kFull, myu, k), 0, 0xFFFFFFFFu);
+    }
+  }
+  cnt = warp_sum_u64(cnt);
+  if (lane == 0 && cnt) atomicAdd(out, cnt);
+}
+
+// ---- C4 -------------------------------------------------------------------
+// Lower-ranked prefix of v's symmetric list below `u`: lower_bound(N(v), u).
+__device__ __forceinline__ uint32_t prefix_below(const uint32_t *l, uint32_t len, uint32_t u) {
+  uint32_t b = 0, e = len;
+  while (b < e) {
+    const uint32_t mid = (b + e) >> 1;
+    if (l[mid] < u) b = mid + 1;
+    else e = mid;
+  }
+  return b;
+}
+
+// Walk every wedge u - v - w with v in N(u), v < u, and w in N(v), w < u,
+// for v = N(u)[k], k in the 32-wide steps kb, kb + kstep, ... < ke; call
+// f(w) for each.  All 32 lanes must call.
+template <typename F>
+__device__ __forceinline__ void c4_wedges(const GraphView &s, const uint32_t *__restrict__ au,
+                                          uint32_t u, uint32_t kb, uint32_t ke, uint32_t kstep,
+                                          int lane, F f) {
+  for (uint32_t k0 = kb; k0 < ke; k0 += kstep) {
+    const uint32_t k = k0 + lane;
+    uint32_t len = 0, base = 0;
+    if (k < ke) {
+      const uint2 rv = s.row[au[k]];
+      base = rv.x;
+      len = prefix_below(s.adj + (uint64_t)rv.x * 4, rv.y, u);
+    }
+    const uint32_t incl = warp_inclusive_sum(len, lane);
+    const uint32_t excl = incl - len;
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    for (uint32_t pb = 0; pb < total; pb += 32) {
+      const uint32_t p = pb + lane;
+      const int o = warp_owner(incl, p);
+      const uint32_t ox = __shfl_sync(kFull, excl, o);
+      const uint32_t ob = __shfl_sync(kFull, base, o);
+      if (p < total) f(s.adj[(uint64_t)ob * 4 + (p - ox)]);
+    }
+  }
+}
+
+// Counter map in shared memory: increments c(w) and returns the old value.
+__device__ __forceinline__ uint32_t map_incr(uint32_t *keys, uint32_t *vals, uint32_t mask, int shift,
+                                             uint32_t w) {
+  uint32_t h = (w * kHashMul) >> shift;
+  while (true) {
+    const uint32_t k = keys[h];
+    if (k == w) return atomicAdd(&vals[h], 1u);
+    if (k == kSentinel) {
+      const uint32_t old = atomicCAS(&keys[h], kSentinel, w);
+      if (old == kSentinel || old == w) return atomicAdd(&vals[h], 1u);
+    }
+    h = (h + 1) & mask;
+  }
+}
+
+__global__ void __launch_bounds__(kPWarps * 32)
+    k_c4_small(GraphView s, const uint32_t *__restrict__ dplus, const uint32_t *__restrict__ light,
+               uint32_t n_light, SchedState *sched, unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) uint32_t sm[];  // kPWarps * 2 * kPSlots words
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *keys = sm + warp * 2 * kPSlots, *vals = keys + kPSlots;
+  unsigned long long acc = 0;
+  while (true) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(&sched->next_warp, 1u);
+    c = __shfl_sync(kFull, c, 0);
+    const uint32_t i0 = c * 32;
+    if (i0 >= n_light) break;
+    const uint32_t nb = min(32u, n_light - i0);
+    const uint32_t myu = lane < nb ? light[i0 + lane] : 0u;
+    for (uint32_t q = 0; q < nb; ++q) {
+      const uint32_t u = __shfl_sync(kFull, myu, q);
+      const uint2 ru = s.row[u];
+      const uint32_t pre = ru.y - dplus[u];  // neighbours ranked below u
+      const uint32_t *au = s.adj + (uint64_t)ru.x * 4;
+      for (uint32_t i = lane; i < kPSlots; i += 32) {
+        keys[i] = kSentinel;
+        vals[i] = 0;
+      }
+      __syncwarp();
+      c4_wedges(s, au, u, 0, pre, 32, lane, [&](uint32_t w) {
+        acc += map_incr(keys, vals, kPSlots - 1, 32 - 10, w);
+      });
+      __syncwarp();
+    }
+  }
+  acc = warp_sum_u64(acc);
+  if (lane == 0 && acc) atomicAdd(out, acc);
+}
+
+// Vertices with more wedges than a warp map holds: the whole CTA walks them
+// against a dense counter array of n words owned by this CTA (pool slot
+// blockIdx.x, all zero between vertices), then walks them again to reset it.
+__global__ void __launch_bounds__(kPWarps * 32)
+    k_c4_big(GraphView s, const uint32_t *__restrict__ dplus, const uint32_t *__restrict__ big,
+             uint32_t n_big, uint32_t *__restrict__ pool, SchedState *sched,
+             unsigned long long *__restrict__ out) {
+  __shared__ uint32_t s_u, s_next;
+  const int lane = threadIdx.x & 31;
+  uint32_t *cnt = pool + (uint64_t)blockIdx.x * s.n;
+  unsigned long long acc = 0;
+  while (true) {
+    if (threadIdx.x == 0) {
+      s_u = atomicAdd(&sched->next_cta, 1u);
+      s_next = 0;
+    }
+    __syncthreads();
+    if (s_u >= n_big) break;
+    const uint32_t u = big[s_u];
+    const uint2 ru = s.row[u];
+    const uint32_t pre = ru.y - dplus[u];
+    const uint32_t *au = s.adj + (uint64_t)ru.x * 4;
+    // pass 1: count, claiming 32 middle vertices at a time
+    while (true) {
+      uint32_t k = 0;
+      if (lane == 0) k = atomicAdd(&s_next, 32u);
+      k = __shfl_sync(kFull, k, 0);
+      if (k >= pre) break;
+      c4_wedges(s, au, u, k, min(k + 32, pre), 32, lane,
+                [&](uint32_t w) { acc += atomicAdd(&cnt[w], 1u); });
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_next = 0;
+    __syncthreads();
+    // pass 2: reset the counters this vertex touched
+    while (true) {
+      uint32_t k = 0;
+      if (lane == 0) k = atomicAdd(&s_next, 32u);
+      k = __shfl_sync(kFull, k, 0);
+      if (k >= pre) break;
+      c4_wedges(s, au, u, k, min(k + 32, pre), 32, lane, [&](uint32_t w) { cnt[w] = 0u; });
+    }
+    __syncthreads();
+  }
+  acc = warp_sum_u64(acc);
+  if (lane == 0 && acc) atomicAdd(out, acc);
+}
+
+// ---- plans ------------------------------------------------------------------
+// K4 per-vertex classes: d+(u) >= 3 needed; CTA when d+(u) > warp capacity.
+__global__ void k_k4_classify(const uint2 *__restrict__ row, const uint64_t *__restrict__ wedge,
+                              uint32_t n, uint64_t tw, uint64_t twc, uint8_t *__restrict__ cls,
+                              uint64_t *__restrict__ costL, uint32_t *__restrict__ kW,
+                              uint32_t *__restrict__ kC) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = row[u].y;
+    uint8_t c = kClassNone;
+    uint64_t cl = 0;
+    uint32_t kw = 0, kc = 0;
+    if (d >= 3) {
+      const uint64_t cost = 3 * wedge[u] + 4 * d + 64;
+      const uint32_t span = d - 2;  // middle positions that can close a clique
+      if (d > kPSlots / 2) {
+        c = kClassCta;
+        kc = (uint32_t)min64((cost + twc - 1) / twc, span);
+      } else if (cost > tw) {
+        c = kClassSplit;
+        kw = (uint32_t)min64((cost + tw - 1) / tw, span);
+      } else {
+        c = kClassLight;
+        cl = cost;
+      }
+    }
+    cls[u] = c;
+    costL[u] = cl;
+    kW[u] = kw;
+    kC[u] = kc;
+  }
+}
+
+__global__ void k_split_tiles(const uint2 *__restrict__ row, uint32_t n,
+                              const uint32_t *__restrict__ off, Tile *__restrict__ tiles) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t kk = off[u + 1] - off[u];
+    if (!kk) continue;
+    const uint32_t span = row[u].y - 2;
+    for (uint32_t i = 0; i < kk; ++i) {
+      Tile t;
+      t.v0 = (uint32_t)u;
+      t.v1 = (uint32_t)u + 1;
+      t.j0 = (uint32_t)((uint64_t)i * span / kk);
+      t.j1 = (uint32_t)((uint64_t)(i + 1) * span / kk);
+      tiles[off[u] + i] = t;
+    }
+  }
+}
+
+__global__ void k_group_tiles(const uint32_t *__restrict__ starts, uint64_t G, uint32_t L,
+                              Tile *__restrict__ tiles) {
+  for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G;
+       g += (uint64_t)gridDim.x * blockDim.x) {
+    Tile t;
+    t.v0 = starts[g];
+    t.v1 = g + 1 < G ? starts[g + 1] : L;
+    t.j0 = 0;
+    t.j1 = kGroupTile;
+    tiles[g] = t;
+  }
+}
+
+struct ClassIs {
+  const uint8_t *cls;
+  uint8_t c;
+  __host__ __device__ bool operator()(uint32_t v) const { return cls[v] == c; }
+};
+struct CostOf {
+  const uint64_t *cost;
+  __host__ __device__ uint64_t operator()(uint32_t v) const { return cost[v]; }
+};
+struct Target {
+  uint64_t tw;
+  __host__ __device__ uint64_t operator()(uint64_t g) const { return g * tw; }
+};
+
+// C4 per-vertex class by an upper bound of its wedge count.
+__global__ void k_c4_classify(const uint2 *__restrict__ srow, const uint32_t *__restrict__ sadj,
+                              const uint32_t *__restrict__ dplus, uint32_t n, uint32_t warp_cap,
+                              uint8_t *__restrict__ cls) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 r = srow[u];
+    const uint32_t pre = r.y - dplus[u];
+    uint64_t w = 0;
+    for (uint32_t k = 0; k < pre && w <= warp_cap; ++k) w += srow[sadj[(uint64_t)r.x * 4 + k]].y;
+    cls[u] = pre == 0 ? kClassNone : (w <= warp_cap ? kClassLight : kClassCta);
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
+  auto plan = std::make_unique<PatternPlan>();
+  const uint32_t n = g->n;
+  auto pol = thrust::cuda::par_nosync.on(s);
+  const uint64_t tw = 1u << 16, twc = 1u << 20;
+  DevBuf<uint8_t> cls;
+  DevBuf<uint64_t> costL;
+  DevBuf<uint32_t> kW, kC;
+  GARY_TRY(cls.alloc(n, s));
+  GARY_TRY(costL.alloc(n, s));
+  GARY_TRY(kW.alloc((uint64_t)n + 1, s));
+  GARY_TRY(kC.alloc((uint64_t)n + 1, s));
+  k_k4_classify<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, g->wedge.p, n, tw, twc, cls.p, costL.p,
+                                                 kW.p, kC.p);
+  GARY_CUDA(cudaGetLastError());
+  GARY_CUDA(cudaMemsetAsync(kW.p + n, 0, 4, s));
+  GARY_CUDA(cudaMemsetAsync(kC.p + n, 0, 4, s));
+  thrust::exclusive_scan(pol, kW.p, kW.p + n + 1, kW.p, 0u);
+  thrust::exclusive_scan(pol, kC.p, kC.p + n + 1, kC.p, 0u);
+  uint32_t nW = 0, nC = 0;
+  GARY_CUDA(cudaMemcpyAsync(&nW, kW.p + n, 4, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaMemcpyAsync(&nC, kC.p + n, 4, cudaMemcpyDeviceToHost, s));
+  GARY_TRY(plan->light.alloc_persistent(std::max<uint32_t>(n, 1)));
+  const uint32_t L = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                                thrust::counting_iterator<uint32_t>(n), plan->light.p,
+                                                ClassIs{cls.p, kClassLight}) - plan->light.p);
+  DevBuf<uint64_t> lc;
+  GARY_TRY(lc.alloc((uint64_t)L + 1, s));
+  auto costs = thrust::make_transform_iterator(plan->light.p, CostOf{costL.p});
+  thrust::exclusive_scan(pol, costs, costs + L, lc.p, 0ull);
+  const uint64_t totalL = L ? thrust::reduce(pol, costs, costs + L, 0ull) : 0;
+  GARY_CUDA(cudaStreamSynchronize(s));
+  const uint64_t G = totalL ? (totalL + tw - 1) / tw : 0;
+  plan->n_cta = nC;
+  plan->n_warp = (uint32_t)(nW + G);
+  GARY_TRY(plan->tiles.alloc_persistent(std::max<uint64_t>((uint64_t)nC + nW + G, 1)));
+  k_split_tiles<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, n, kC.p, plan->tiles.p);
+  k_split_tiles<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, n, kW.p, plan->tiles.p + nC);
+  if (G) {
+    DevBuf<uint32_t> starts;
+    GARY_TRY(starts.alloc(G, s));
+    auto tg = thrust::make_transform_iterator(thrust::counting_iterator<uint64_t>(0), Target{tw});
+    thrust::lower_bound(pol, lc.p, lc.p + L, tg, tg + G, starts.p);
+    k_group_tiles<<<grid_for(G), kThreads, 0, s>>>(starts.p, G, L, plan->tiles.p + nC + nW);
+  }
+  GARY_CUDA(cudaGetLastError());
+  GARY_TRY(plan->sched.alloc_persistent(1));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  *out = plan.release();
+  return GARY_OK;
+}
+
+int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaStream_t s,
+              uint32_t shard, uint32_t nshards) {
+  const size_t smem = (size_t)2 * kCtaSlots * 4;  // >= kPWarps * 2 * kPSlots words
+  static_assert(2 * kCtaSlots >= kPWarps * 2 * kPSlots, "shared buffer too small for warp tables");
+  static bool attr[64] = {false};
+  const int dev = device_ordinal();
+  if (dev < 64 && !attr[dev]) {
+    GARY_CUDA(cudaFuncSetAttribute(k_k4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr[dev] = true;
+  }
+  int per_sm = 0;
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_k4, kPWarps * 32, smem));
+  if (per_sm < 1) per_sm = 1;
+  const TileRange rng = shard_range(plan->n_cta, plan->n_warp, shard, nshards);
+  GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
+  GARY_CUDA(cudaMemsetAsync(d_out, 0, 8, s));
+  GARY_CUDA(cudaEventRecord(g->ev0, s));
+  k_k4<<<(unsigned)(sm_count() * per_sm), kPWarps * 32, smem, s>>>(
+      g->view(), plan->tiles.p, plan->light.p, plan->n_cta, rng, plan->sched.p, d_out);
+  GARY_CUDA(cudaGetLastError());
+  GARY_CUDA(cudaEventRecord(g->ev1, s));
+  g->last = gary_count_stats{};
+  g->last.tiles = (rng.cta_hi - rng.cta_lo) + (rng.warp_hi - rng.warp_lo);
+  g->last.cta_tiles = rng.cta_hi - rng.cta_lo;
+  g->last_timed = true;
+  return GARY_OK;
+}
+
+int build_c4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
+  GARY_TRY(build_symmetric(g, s));
+  auto plan = std::make_unique<PatternPlan>();
+  const uint32_t n = g->n;
+  auto pol = thrust::cuda::par_nosync.on(s);
+  DevBuf<uint8_t> cls;
+  GARY_TRY(cls.alloc(n, s));
+  k_c4_classify<<<grid_for(n), kThreads, 0, s>>>(g->sym.row.p, g->sym.adj.p, g->dag.outdeg.p, n,
+                                                 kPSlots / 2, cls.p);
+  GARY_CUDA(cudaGetLastError());
+  GARY_TRY(plan->light.alloc_persistent(std::max<uint32_t>(n, 1)));
+  GARY_TRY(plan->big.alloc_persistent(std::max<uint32_t>(n, 1)));
+  plan->n_light = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                             thrust::counting_iterator<uint32_t>(n), plan->light.p,
+                                             ClassIs{cls.p, kClassLight}) - plan->light.p);
+  plan->n_big = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                           thrust::counting_iterator<uint32_t>(n), plan->big.p,
+                                           ClassIs{cls.p, kClassCta}) - plan->big.p);
+  plan->pool_ctas = std::min<uint32_t>(plan->n_big, (uint32_t)sm_count());
+  if (plan->pool_ctas) {
+    GARY_TRY(plan->pool.alloc_persistent((uint64_t)plan->pool_ctas * n));
+    GARY_CUDA(cudaMemsetAsync(plan->pool.p, 0, plan->pool.bytes(), s));
+  }
+  GARY_TRY(plan->sched.alloc_persistent(1));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  *out = plan.release();
+  return GARY_OK;
+}
+
+int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaStream_t s,
+              uint32_t shard, uint32_t nshards) {
+  // shards split the light list and the big list
+  const uint32_t l0 = (uint32_t)((uint64_t)plan->n_light * shard / nshards);
+  const uint32_t l1 = (uint32_t)((uint64_t)plan->n_light * (shard + 1) / nshards);
+  const uint32_t b0 = (uint32_t)((uint64_t)plan->n_big * shard / nshards);
+  const uint32_t b1 = (uint32_t)((uint64_t)plan->n_big * (shard + 1) / nshards);
+  const size_t smem = (size_t)kPWarps * 2 * kPSlots * 4;
+  static bool attr[64] = {false};
+  const int dev = device_ordinal();
+  if (dev < 64 && !attr[dev]) {
+    GARY_CUDA(cudaFuncSetAttribute(k_c4_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr[dev] = true;
+  }
+  int per_sm = 0;
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_small, kPWarps * 32, smem));
+  if (per_sm < 1) per_sm = 1;
+  const GraphView sv{g->n, g->sym.row.p, g->sym.adj.p, true};
+  GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
+  GARY_CUDA(cudaMemsetAsync(d_out, 0, 8, s));
+  GARY_CUDA(cudaEventRecord(g->ev0, s));
+  if (b1 > b0)
+    k_c4_big<<<std::min<uint32_t>(plan->pool_ctas, b1 - b0), kPWarps * 32, 0, s>>>(
+        sv, g->dag.outdeg.p, plan->big.p + b0, b1 - b0, plan->pool.p, plan->sched.p, d_out);
+  if (l1 > l0)
+    k_c4_small<<<(unsigned)(sm_count() * per_sm), kPWarps * 32, smem, s>>>(
+        sv, g->dag.outdeg.p, plan->light.p + l0, l1 - l0, plan->sched.p, d_out);
+  GARY_CUDA(cudaGetLastError());
+  GARY_CUDA(cudaEventRecord(g->ev1, s));
+  g->last = gary_count_stats{};
+  g->last.tiles = (l1 - l0) + (b1 - b0);
+  g->last.cta_tiles = b1 - b0;
+  g->last_timed = true;
+  return GARY_OK;
+}
+
+}  // namespace gary

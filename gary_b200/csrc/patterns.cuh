@@ -1,0 +1,29 @@
+// Plans and launches of the 4-clique and 4-cycle kernels (patterns.cu).
+#pragma once
+#include <cstdint>
+
+#include "graph.cuh"
+#include "tc.cuh"
+
+namespace gary {
+
+// Largest d+(u) the 4-clique kernel supports (a CTA-wide table of 8192 slots).
+constexpr uint32_t kK4MaxOutDegree = 4096;
+
+struct PatternPlan {
+  DevBuf<Tile> tiles;      // K4: CTA tiles then warp tiles
+  DevBuf<uint32_t> light;  // light vertices (K4 groups index it; C4 warps walk it)
+  DevBuf<uint32_t> big;    // C4: vertices walked by a whole CTA
+  DevBuf<uint32_t> pool;   // C4: pool_ctas dense counter arrays of n words
+  DevBuf<SchedState> sched;
+  uint32_t n_cta = 0, n_warp = 0, n_light = 0, n_big = 0, pool_ctas = 0;
+};
+
+int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out);
+int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaStream_t s,
+              uint32_t shard, uint32_t nshards);
+int build_c4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out);
+int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaStream_t s,
+              uint32_t shard, uint32_t nshards);
+
+}  // namespace gary

@@ -1,0 +1,81 @@
+"""4-cycle and 4-clique counts on the GPU against the CPU oracle and
+closed-form known answers (the reference has no implementation of these
+patterns: rectCountHom is declared only, include/kernels/GraphQueryHom.cuh:48)."""
+from __future__ import annotations
+
+import itertools
+from math import comb
+
+import numpy as np
+import pytest
+
+import gary_b200 as gb
+from gary_b200 import _lib
+from graphs import edges_of
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+K3, C4, K4 = _lib.GARY_PATTERN_TRIANGLE, _lib.GARY_PATTERN_4CYCLE, _lib.GARY_PATTERN_4CLIQUE
+
+
+def _graph(n, edges):
+    e = np.array(edges, np.uint32).reshape(-1, 2)
+    ptr, idx = O.sym_csr(e[:, 0], e[:, 1], n)
+    return ptr, idx
+
+
+def _counts(ptr, idx, n):
+    with gb.Graph.upload(ptr, idx, n) as g:
+        return g.count(K3), g.count(C4), g.count(K4)
+
+
+@pytest.mark.parametrize("n", [4, 5, 8, 13, 40])
+def test_complete_graphs(cuda, n):
+    ptr, idx = _graph(n, list(itertools.combinations(range(n), 2)))
+    assert _counts(ptr, idx, n) == (comb(n, 3), 3 * comb(n, 4), comb(n, 4))
+
+
+def test_small_kats(cuda):
+    assert _counts(*_graph(17, [(0, i) for i in range(1, 17)]), 17) == (0, 0, 0)
+    assert _counts(*_graph(4, [(0, 1), (1, 2), (2, 3), (3, 0)]), 4) == (0, 1, 0)
+    wheel = [(0, i) for i in range(1, 11)] + [(i, i % 10 + 1) for i in range(1, 11)]
+    assert _counts(*_graph(11, wheel), 11) == (10, 10, 0)
+    assert _counts(*_graph(5, [(0, 2), (0, 3), (0, 4), (1, 2), (1, 3), (1, 4)]), 5) == (0, 3, 0)
+    assert _counts(*_graph(6, []), 6) == (0, 0, 0)
+    # complete bipartite K_{30,40}: C(30,2) C(40,2) 4-cycles, no triangles
+    kb = [(a, 30 + b) for a in range(30) for b in range(40)]
+    assert _counts(*_graph(70, kb), 70) == (0, comb(30, 2) * comb(40, 2), 0)
+
+
+def test_golden_graphs_vs_oracle(golden, cuda):
+    for case in golden["graphs"]:
+        if case["sym_nnz"] > 2_000_000:
+            continue
+        n, src, dst = edges_of(case)
+        ptr, idx = O.sym_csr(src, dst, n)
+        dptr, didx = O.orient(ptr, idx)
+        want = (case["ref_triangles"], O.c4_count(ptr, idx), O.k4_count(dptr, didx))
+        assert _counts(ptr, idx, n) == want, case["name"]
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(16, 16, 3), (18, 8, 4)])
+def test_rmat_vs_oracle(cuda, scale, ef, seed):
+    n = 1 << scale
+    src, dst = gb.gen_rmat(scale, seed, ef << scale)
+    ptr, idx = gb.csr_from_edges(src, dst, n)
+    dptr, didx = O.orient(ptr, idx)
+    with gb.Graph.upload(ptr, idx, n) as g:
+        assert g.count(C4) == O.c4_count(ptr, idx)
+        assert g.count(K4) == O.k4_count(dptr, didx)
+        # counting again reuses the cached plans and gives the same numbers
+        assert g.count(C4) == O.c4_count(ptr, idx)
+
+
+def test_c4_trace_identity_on_gpu(cuda):
+    """hom(C4) = tr(A^4) = 8 C4 + 2 sum d(d-1) + 2m, with C4 from the GPU."""
+    src, dst = gb.gen_rmat(12, 9, 16 << 12)
+    ptr, idx = gb.csr_from_edges(src, dst, 1 << 12)
+    d = np.diff(ptr.astype(np.int64))
+    with gb.Graph.upload(ptr, idx, 1 << 12) as g:
+        c4 = g.count(C4)
+    assert O.c4_hom(ptr, idx) == 8 * c4 + 2 * int((d * (d - 1)).sum()) + int(d.sum())
