@@ -105,6 +105,16 @@ SIGNATURES = {
     "gary_count_last_stats": (_INT, [_P, C.POINTER(CountStats)]),
     "gary_count_triangles_noalloc": (_INT, [_P, _P, _P, _U32, _P, _P]),
     "gary_tune": (_INT, [C.c_char_p, _U64]),
+    "gary_mlp_param_count": (_INT, []),
+    "gary_mlp_init": (_INT, [_U64, _P]),
+    "gary_mlp_forward": (_INT, [_P, _P, _U64, _INT, _P, _P]),
+    "gary_mlp_grad": (_INT, [_P, _P, _P, _P, _U64, C.c_float, _P, _P, _P]),
+    "gary_mlp_adam": (_INT, [_P, _P, _P, _P, _U32, C.c_float, _P]),
+    "gary_mlp_save": (_INT, [C.c_char_p, _P]),
+    "gary_mlp_load": (_INT, [C.c_char_p, _P]),
+    "gary_set_cost_model": (_INT, [_P]),
+    "gary_tc_features": (_INT, [_P, _P, _P, _P]),
+    "gary_tc_profile": (_INT, [_P, _INT, _P, _P, _P]),
     "gary_intersect_batch": (_INT, [_U64, _P, _P, _P, _P, _P, _P, _INT, _P, _P, _P, _P, _P, _P]),
     "gary_search_batch": (_INT, [_P, _U64, _P, _U64, _U32, _P, _P, _P]),
     "gary_zipf_table": (_INT, [_U32, C.c_double, _P]),

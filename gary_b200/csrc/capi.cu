@@ -9,9 +9,11 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "graph.cuh"
 #include "internal.cuh"
+#include "mlp.cuh"
 #include "patterns.cuh"
 #include "tc.cuh"
 
@@ -87,6 +89,8 @@ int plan_slot(int pattern, int sched) { return (pattern - 3) * 2 + sched; }
 
 PlanParams g_tuning;  // process-wide knobs of the counting plans (gary_tune)
 std::mutex g_tuning_mu;
+std::vector<float> g_model;  // process-wide cost model (gary_set_cost_model)
+std::mutex g_model_mu;
 
 int count_async(gary_graph *g, int pattern, int sched, cudaStream_t s, unsigned long long *d_out,
                 uint32_t shard = 0, uint32_t nshards = 1) {
@@ -111,12 +115,23 @@ int count_async(gary_graph *g, int pattern, int sched, cudaStream_t s, unsigned 
     if (!g->c4_plan) GARY_TRY(build_c4_plan(g, s, &g->c4_plan));
     return launch_c4(g, g->c4_plan, d_out, s, shard, nshards);
   }
-  if (sched != GARY_SCHED_PLAIN) {
-    set_error("scheduler %d is not available in this build", sched);
-    return GARY_ERR_UNSUPPORTED;
-  }
   const int slot = plan_slot(pattern, sched);
-  if (!g->plans[slot]) GARY_TRY(build_k3_plan(g, tuned_params(), s, &g->plans[slot]));
+  if (!g->plans[slot]) {
+    if (sched == GARY_SCHED_LEARNED) {
+      std::vector<float> model;
+      {
+        std::lock_guard<std::mutex> lk(g_model_mu);
+        model = g_model;
+      }
+      if (model.empty()) {
+        set_error("GARY_SCHED_LEARNED needs a cost model: call gary_set_cost_model first");
+        return GARY_ERR_INVALID;
+      }
+      GARY_TRY(build_k3_plan(g, tuned_params(), s, &g->plans[slot], model.data()));
+    } else {
+      GARY_TRY(build_k3_plan(g, tuned_params(), s, &g->plans[slot]));
+    }
+  }
   return launch_k3(g, g->plans[slot], d_out, s, shard, nshards);
 }
 
@@ -147,6 +162,46 @@ extern "C" int gary_tune(const char *key, uint64_t value) {
     return GARY_ERR_INVALID;
   }
   return GARY_OK;
+}
+
+extern "C" int gary_set_cost_model(const float *params) {
+  std::lock_guard<std::mutex> lk(gary::g_model_mu);
+  if (!params) {
+    gary::g_model.clear();
+    return GARY_OK;
+  }
+  gary::g_model.assign(params, params + gary::kMlpParams);
+  return GARY_OK;
+}
+
+extern "C" int gary_tc_features(gary_graph *g, float *d_x, uint8_t *d_legal, void *stream) {
+  GARY_CHECK_ARG(g && d_x && d_legal, "NULL argument");
+  return guarded("gary_tc_features", [&] {
+    cudaStream_t s = gary::as_stream(stream);
+    const int slot = gary::plan_slot(GARY_PATTERN_TRIANGLE, GARY_SCHED_PLAIN);
+    if (!g->plans[slot]) GARY_TRY(gary::build_k3_plan(g, gary::tuned_params(), s, &g->plans[slot]));
+    return gary::k3_features(g, g->plans[slot], d_x, d_legal, s);
+  });
+}
+
+extern "C" int gary_tc_profile(gary_graph *g, int variant, uint64_t *d_cycles, uint64_t *d_count,
+                               void *stream) {
+  GARY_CHECK_ARG(g && d_cycles && d_count, "NULL argument");
+  GARY_CHECK_ARG(variant >= -1 && variant <= 3, "variant must be -1 (plain) or 0..3");
+  return guarded("gary_tc_profile", [&] {
+    cudaStream_t s = gary::as_stream(stream);
+    const int slot = gary::plan_slot(GARY_PATTERN_TRIANGLE, GARY_SCHED_PLAIN);
+    if (!g->plans[slot]) GARY_TRY(gary::build_k3_plan(g, gary::tuned_params(), s, &g->plans[slot]));
+    gary::DevBuf<uint8_t> forced;
+    if (variant >= 0) {
+      GARY_TRY(forced.alloc(g->n, s));
+      GARY_CUDA(cudaMemsetAsync(forced.p, variant, g->n, s));
+    }
+    GARY_CUDA(cudaMemsetAsync(d_cycles, 0, (uint64_t)g->n * 8, s));
+    return gary::launch_k3_ctl(g, g->plans[slot], reinterpret_cast<unsigned long long *>(d_count), s,
+                               0, 1, variant >= 0 ? forced.p : nullptr,
+                               reinterpret_cast<unsigned long long *>(d_cycles));
+  });
 }
 
 extern "C" int gary_graph_drop_plans(gary_graph *g) {

@@ -98,11 +98,13 @@ __global__ void k_row_heads(const uint64_t *__restrict__ ptr, uint32_t n,
   }
 }
 
-__global__ void k_rank_scatter(const uint32_t *__restrict__ perm, uint32_t n,
-                               uint32_t *__restrict__ rank) {
+__global__ void k_rank_scatter(const uint32_t *__restrict__ perm, const uint32_t *__restrict__ deg,
+                               uint32_t n, uint32_t *__restrict__ rank, uint32_t *__restrict__ rdeg) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
+       i += (uint64_t)gridDim.x * blockDim.x) {
     rank[perm[i]] = (uint32_t)i;
+    rdeg[i] = deg[perm[i]];
+  }
 }
 
 __device__ __forceinline__ bool before(uint32_t a, uint32_t b, const uint32_t *deg) {
@@ -394,7 +396,8 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
     GARY_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kb, vb, n, 0, eb, s));
     if (vb.Current() != g->perm.p) std::swap(g->perm, perm2);
     GARY_TRY(rank.alloc(n, s));
-    k_rank_scatter<<<grid_for(n), kThreads, 0, s>>>(g->perm.p, n, rank.p);
+    GARY_TRY(g->rdeg.alloc_persistent(n));
+    k_rank_scatter<<<grid_for(n), kThreads, 0, s>>>(g->perm.p, deg.p, n, rank.p, g->rdeg.p);
     GARY_CUDA(cudaGetLastError());
   }
 

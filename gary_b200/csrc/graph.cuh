@@ -56,6 +56,7 @@ struct gary_graph {
   gary::PaddedCSR kept;          // caller ids (GARY_KEEP_IDS only)
   gary::DevBuf<uint64_t> wedge;  // per vertex: sum of d+(w) over w in N+(v)
   gary::DevBuf<uint32_t> perm;   // rank -> caller id
+  gary::DevBuf<uint32_t> rdeg;   // undirected degree by rank id (cost-model feature)
 
   // symmetric ranked lists (built lazily for 4-cycle counting)
   gary::PaddedCSR sym;
@@ -71,7 +72,7 @@ struct gary_graph {
   gary::GraphView view() const { return gary::GraphView{n, dag.row.p, dag.adj.p, true}; }
   gary::PaddedCSR &user_view() { return keep_ids ? kept : dag; }
   uint64_t device_bytes() const {
-    return dag.bytes() + kept.bytes() + sym.bytes() + wedge.bytes() + perm.bytes();
+    return dag.bytes() + kept.bytes() + sym.bytes() + wedge.bytes() + perm.bytes() + rdeg.bytes();
   }
 };
 

@@ -35,6 +35,7 @@
 #include <memory>
 
 #include "bulk.cuh"
+#include "mlp.cuh"
 #include "graph.cuh"
 #include "tc.cuh"
 #include "warp_ops.cuh"
@@ -118,9 +119,12 @@ __global__ void k_in_work(const uint32_t *__restrict__ keys, const uint2 *__rest
   }
 }
 
+// pcost (optional): predicted cycles of a warp-class vertex, with tile target
+// tw_pred in the same unit; without it, costs are probe counts.
 __global__ void k_classify(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
                            const uint64_t *__restrict__ work,
                            const uint64_t *__restrict__ inptr, uint32_t n, PlanParams pp,
+                           const uint64_t *__restrict__ pcost, uint64_t tw_pred,
                            uint8_t *__restrict__ vclass, uint64_t *__restrict__ costL,
                            uint32_t *__restrict__ kW, uint32_t *__restrict__ kC) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
@@ -138,13 +142,15 @@ __global__ void k_classify(const uint2 *__restrict__ row, const uint32_t *__rest
       const bool bitmap = span <= bitmap_max_span(kWarpTableSlots);
       const bool warp_fits = bitmap || dv <= pp.warp_cap;
       const uint64_t build = bitmap ? (span >> 5) + dv : 4ull * dv;
-      const uint64_t c = work[v] + build + pp.vertex_overhead;
+      const bool pred = pcost && warp_fits;
+      const uint64_t c = pred ? pcost[v] + 1 : work[v] + build + pp.vertex_overhead;
+      const uint64_t tw = pred ? tw_pred : pp.warp_tile_cost;
       if (!warp_fits) {
         cls = kClassCta;
         kc = (uint32_t)min_u64((c + pp.cta_tile_cost - 1) / pp.cta_tile_cost, nin);
-      } else if (c > pp.warp_tile_cost) {
+      } else if (c > tw) {
         cls = kClassSplit;
-        kw = (uint32_t)min_u64((c + pp.warp_tile_cost - 1) / pp.warp_tile_cost, nin);
+        kw = (uint32_t)min_u64((c + tw - 1) / tw, nin);
       } else {
         cls = kClassLight;
         cl = c;
@@ -208,6 +214,79 @@ __global__ void k_fill_group_tiles(const uint32_t *__restrict__ starts, uint64_t
   }
 }
 
+}  // namespace
+
+// Cost-model features of middle vertex v (all log2(1 + .)):
+//   x0 degree, x1 mean in-edge suffix length (the other endpoints' remaining
+//   out-degree), x2 = x0 - x1 (their log ratio), x3 out-degree d+(v),
+//   x4 id span of N+(v), x5 number of in-edge records.
+// legal[v]: bit k when variant k can run v on a warp (0: not a warp vertex).
+__global__ void k_features(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
+                           const uint32_t *__restrict__ rdeg, const uint64_t *__restrict__ work,
+                           const uint64_t *__restrict__ inptr, uint32_t n, uint32_t warp_cap,
+                           float *__restrict__ x, uint8_t *__restrict__ legal) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 rv = row[v];
+    const uint32_t d = rv.y;
+    const uint64_t nin = inptr[v + 1] - inptr[v];
+    const uint32_t span = d ? adj[(uint64_t)rv.x * 4 + d - 1] - adj[(uint64_t)rv.x * 4] : 0u;
+    const bool warp_fits = span <= bitmap_max_span(kWarpTableSlots) || d <= warp_cap;
+    uint32_t lg = 0;
+    if (d && nin && warp_fits)
+      for (uint32_t k = 0; k < 4; ++k)
+        if (variant_legal(k, d, span)) lg |= 1u << k;
+    legal[v] = (uint8_t)lg;
+    const float x0 = log2f(1.f + (float)rdeg[v]);
+    const float x1 = log2f(1.f + (float)work[v] / (float)(nin ? nin : 1));
+    float *xv = x + v * kMlpIn;
+    xv[0] = x0;
+    xv[1] = x1;
+    xv[2] = x0 - x1;
+    xv[3] = log2f(1.f + (float)d);
+    xv[4] = log2f(1.f + (float)span);
+    xv[5] = log2f(1.f + (float)nin);
+  }
+}
+
+// The cost model over every warp vertex: variant = argmin over legal
+// variants of predicted log2 cycles, pcost = predicted cycles of that variant.
+__global__ void k_predict(const float *__restrict__ params, const float *__restrict__ x,
+                          const uint8_t *__restrict__ legal, uint32_t n, uint8_t *__restrict__ variant,
+                          uint64_t *__restrict__ pcost) {
+  __shared__ float P[kMlpParams];
+  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) P[i] = params[i];
+  __syncthreads();
+  float h1[kMlpH1], h2[kMlpH2];
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t lg = legal[v];
+    if (!lg) {
+      variant[v] = 0xFF;
+      pcost[v] = 0;
+      continue;
+    }
+    float xi[kMlpIn], y[kMlpOut];
+#pragma unroll
+    for (int f = 0; f < kMlpIn; ++f) xi[f] = (x[v * kMlpIn + f] - P[kMlpMuX + f]) / P[kMlpSdX + f];
+    mlp_forward_one(P, xi, h1, h2, y);
+    uint32_t best = 0xFF;
+    float by = 0.f;
+#pragma unroll
+    for (int k = 0; k < kMlpOut; ++k) {
+      const float yk = y[k] * P[kMlpSdY + k] + P[kMlpMuY + k];
+      if (((lg >> k) & 1) && (best == 0xFF || yk < by)) {
+        best = k;
+        by = yk;
+      }
+    }
+    variant[v] = (uint8_t)best;
+    pcost[v] = (uint64_t)exp2f(fminf(fmaxf(by, 0.f), 40.f));
+  }
+}
+
+namespace {
+
 int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
   const uint32_t n = g->n;
   const uint64_t W = g->dag.words;
@@ -266,7 +345,8 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
 
 }  // namespace
 
-int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_count_plan **out) {
+int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_count_plan **out,
+                  const float *model) {
   auto plan = std::make_unique<gary_count_plan>();
   plan->params = pp;
   const uint32_t n = g->n;
@@ -278,8 +358,31 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
   GARY_TRY(costV.alloc(n, s));
   GARY_TRY(kW.alloc((uint64_t)n + 1, s));
   GARY_TRY(kC.alloc((uint64_t)n + 1, s));
+  // learned plans: per-vertex features -> cost model -> variant and predicted cycles
+  DevBuf<uint64_t> pcost;
+  uint64_t tw = pp.warp_tile_cost;
+  if (model) {
+    DevBuf<float> x, dmodel;
+    DevBuf<uint8_t> legal;
+    GARY_TRY(x.alloc((uint64_t)n * kMlpIn, s));
+    GARY_TRY(legal.alloc(n, s));
+    GARY_TRY(dmodel.alloc(kMlpParams, s));
+    GARY_TRY(pcost.alloc(n, s));
+    GARY_TRY(plan->variant.alloc_persistent(n));
+    GARY_CUDA(cudaMemcpyAsync(dmodel.p, model, kMlpParams * 4, cudaMemcpyHostToDevice, s));
+    k_features<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, g->rdeg.p, plan->in.work.p,
+                                                plan->in.inptr.p, n, pp.warp_cap, x.p, legal.p);
+    k_predict<<<grid_for(n), 128, 0, s>>>(dmodel.p, x.p, legal.p, n, plan->variant.p, pcost.p);
+    GARY_CUDA(cudaGetLastError());
+    const uint64_t total = thrust::reduce(pol, pcost.p, pcost.p + n, 0ull);
+    // about 48 warp tiles per resident warp
+    const uint64_t slots = (uint64_t)sm_count() * 2 * kTcWarps * 48;
+    tw = std::max<uint64_t>(total / std::max<uint64_t>(slots, 1), 4096);
+    plan->learned = true;
+  }
   k_classify<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, plan->in.work.p, plan->in.inptr.p, n, pp,
-                                              plan->vclass.p, costV.p, kW.p, kC.p);
+                                              model ? pcost.p : nullptr, tw, plan->vclass.p, costV.p, kW.p,
+                                              kC.p);
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaMemsetAsync(kW.p + n, 0, 4, s));
   GARY_CUDA(cudaMemsetAsync(kC.p + n, 0, 4, s));
@@ -290,7 +393,7 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
   GARY_CUDA(cudaMemcpyAsync(&nW, kW.p + n, 4, cudaMemcpyDeviceToHost, s));
   GARY_CUDA(cudaMemcpyAsync(&nC, kC.p + n, 4, cudaMemcpyDeviceToHost, s));
   GARY_CUDA(cudaStreamSynchronize(s));
-  const uint64_t G = totalL ? (totalL + pp.warp_tile_cost - 1) / pp.warp_tile_cost : 0;
+  const uint64_t G = totalL ? (totalL + tw - 1) / tw : 0;
   const uint64_t total = (uint64_t)nC + nW + G;
   if (total >= (1ull << 31)) {
     set_error("tile plan too large (%llu tiles)", (unsigned long long)total);
@@ -318,7 +421,7 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
     DevBuf<uint32_t> starts;
     GARY_TRY(starts.alloc(G, s));
     auto targets = thrust::make_transform_iterator(thrust::counting_iterator<uint64_t>(0),
-                                                   GroupTarget{pp.warp_tile_cost});
+                                                   GroupTarget{tw});
     thrust::lower_bound(pol, lc.p, lc.p + L, targets, targets + G, starts.p);
     k_fill_group_tiles<<<grid_for(G), kThreads, 0, s>>>(starts.p, G, L, plan->tiles.p + nC + nW);
     GARY_CUDA(cudaGetLastError());
@@ -483,11 +586,49 @@ __device__ uint32_t cta_tile(const GraphView &g, const uint2 *__restrict__ inedg
   return cnt;
 }
 
+// Sorted copy of N+(v) in shared memory, binary-searched (variant SEARCH).
+struct SmemSearchSet {
+  const uint32_t *list;
+  uint32_t d, lo, span;
+  __device__ __forceinline__ uint32_t contains(uint32_t x) const {
+    if (x - lo > span) return 0;
+    uint32_t b = 0, e = d;
+    while (b < e) {
+      const uint32_t m = (b + e) >> 1;
+      const uint32_t v = list[m];
+      if (v == x) return 1;
+      if (v < x) b = m + 1;
+      else e = m;
+    }
+    return 0;
+  }
+};
+
+// Up to 8 ids held in registers, compared directly (variant MERGE: a merge
+// against a list short enough to keep whole in every lane).
+struct RegSet8 {
+  uint32_t r[8];
+  __device__ __forceinline__ uint32_t contains(uint32_t x) const {
+    uint32_t f = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) f |= (x == r[k]) ? 1u : 0u;
+    return f;
+  }
+};
+
+// Per-vertex control of the warp path; null pointers give the plain
+// dispatch (bitmap when the span fits, else buckets) and no cycle log.
+struct VertexCtl {
+  const uint8_t *variant;      // intersection variant per middle vertex
+  unsigned long long *cycles;  // clock64 cycles spent per middle vertex
+};
+
 // One middle vertex v on one warp: a set of N+(v) in the warp's slots, walk
 // in-edges [j0, j1) of v.
 __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 *__restrict__ inedge,
                                                 const uint64_t *__restrict__ inptr, uint32_t v,
-                                                uint32_t j0, uint32_t j1, uint32_t *tab, int lane) {
+                                                uint32_t j0, uint32_t j1, uint32_t *tab, int lane,
+                                                const VertexCtl &ctl) {
   const uint2 rv = g.row[v];
   const uint32_t d = rv.y;
   const uint64_t base = inptr[v];
@@ -495,19 +636,36 @@ __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 
   const uint64_t ke = base + min_u64(j1, nin);
   const uint64_t kb = base + j0;
   if (d == 0 || kb >= ke) return 0;
+  const long long t0 = ctl.cycles ? clock64() : 0;
   const uint32_t *av = g.adj + (uint64_t)rv.x * 4;
   const uint4 *adj4 = reinterpret_cast<const uint4 *>(g.adj);
   const uint32_t lo = av[0], span = av[d - 1] - lo;
   auto sync = [] { __syncwarp(); };
+  uint32_t var = span <= kWarpBitmapSpan ? kVarBitmap : kVarHash;
+  if (ctl.variant) {
+    const uint32_t f = ctl.variant[v];
+    if (variant_legal(f, d, span)) var = f;
+  }
   uint32_t c;
-  if (span <= kWarpBitmapSpan) {
+  if (var == kVarBitmap) {
     const BitmapSet st = build_bitmap(av, d, lo, span, tab, lane, 32, sync);
     c = walk_range(adj4, inedge, kb, ke, lane, st);
-  } else {
+  } else if (var == kVarHash) {
     const BucketSet st = build_buckets(av, d, lo, span, tab, kWarpTableSlots, lane, 32, sync);
+    c = walk_range(adj4, inedge, kb, ke, lane, st);
+  } else if (var == kVarSearch) {
+    for (uint32_t i = lane; i < d; i += 32) tab[i] = av[i];
+    __syncwarp();
+    const SmemSearchSet st{tab, d, lo, span};
+    c = walk_range(adj4, inedge, kb, ke, lane, st);
+  } else {
+    RegSet8 st;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) st.r[k] = (uint32_t)k < d ? av[k] : kSentinel;
     c = walk_range(adj4, inedge, kb, ke, lane, st);
   }
   __syncwarp();
+  if (ctl.cycles && lane == 0) atomicAdd(&ctl.cycles[v], (unsigned long long)(clock64() - t0));
   return c;
 }
 
@@ -515,7 +673,7 @@ template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     k_tc_mid(GraphView g, const uint2 *__restrict__ inedge, const uint64_t *__restrict__ inptr,
              const uint32_t *__restrict__ light, const Tile *__restrict__ tiles, uint32_t n_cta,
-             TileRange rng, SchedState *sched, unsigned long long *__restrict__ out) {
+             TileRange rng, SchedState *sched, unsigned long long *__restrict__ out, VertexCtl ctl) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint64_t bar;
   __shared__ uint32_t s_tile, s_chunk;
@@ -550,7 +708,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     if (t >= rng.warp_hi) break;
     const Tile tl = wt[t];
     if (tl.j1 != kGroupTile) {
-      cnt += warp_vertex(g, inedge, inptr, tl.v0, tl.j0, tl.j1, tab, lane);
+      cnt += warp_vertex(g, inedge, inptr, tl.v0, tl.j0, tl.j1, tab, lane, ctl);
       continue;
     }
     // a group of light vertices: list positions [v0, v1), 32 ids per load
@@ -558,7 +716,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
       const uint32_t nb = min(32u, tl.v1 - ib);
       const uint32_t myv = lane < nb ? light[ib + lane] : 0u;
       for (uint32_t k = 0; k < nb; ++k)
-        cnt += warp_vertex(g, inedge, inptr, __shfl_sync(kFull, myv, k), 0, 0xFFFFFFFFu, tab, lane);
+        cnt += warp_vertex(g, inedge, inptr, __shfl_sync(kFull, myv, k), 0, 0xFFFFFFFFu, tab, lane,
+                           ctl);
     }
   }
 
@@ -569,9 +728,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
 
 }  // namespace
 
+int k3_features(gary_graph *g, gary_count_plan *plan, float *d_x, uint8_t *d_legal, cudaStream_t s) {
+  k_features<<<grid_for(g->n), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, g->rdeg.p,
+                                                 plan->in.work.p, plan->in.inptr.p, g->n,
+                                                 plan->params.warp_cap, d_x, d_legal);
+  GARY_CUDA(cudaGetLastError());
+  return GARY_OK;
+}
+
 template <int MINB>
 int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
-                   uint32_t shard, uint32_t nshards) {
+                   uint32_t shard, uint32_t nshards, VertexCtl ctl) {
   constexpr int WARPS = kTcWarps;
   auto kern = k_tc_mid<WARPS, MINB>;
   const size_t smem = (size_t)WARPS * kWarpTableSlots * 4;
@@ -590,7 +757,7 @@ int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_o
   GARY_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), s));
   GARY_CUDA(cudaEventRecord(g->ev0, s));
   kern<<<grid, WARPS * 32, smem, s>>>(g->view(), plan->in.inedge.p, plan->in.inptr.p, plan->light.p,
-                                      plan->tiles.p, plan->n_cta, rng, plan->sched.p, d_out);
+                                      plan->tiles.p, plan->n_cta, rng, plan->sched.p, d_out, ctl);
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
@@ -600,10 +767,17 @@ int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_o
   return GARY_OK;
 }
 
+int launch_k3_ctl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
+                  uint32_t shard, uint32_t nshards, const uint8_t *variant,
+                  unsigned long long *cycles) {
+  const VertexCtl ctl{variant, cycles};
+  if (plan->params.min_blocks >= 3) return launch_k3_impl<3>(g, plan, d_out, s, shard, nshards, ctl);
+  return launch_k3_impl<2>(g, plan, d_out, s, shard, nshards, ctl);
+}
+
 int launch_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
               uint32_t shard, uint32_t nshards) {
-  if (plan->params.min_blocks >= 3) return launch_k3_impl<3>(g, plan, d_out, s, shard, nshards);
-  return launch_k3_impl<2>(g, plan, d_out, s, shard, nshards);
+  return launch_k3_ctl(g, plan, d_out, s, shard, nshards, plan->variant.p, nullptr);
 }
 
 }  // namespace gary

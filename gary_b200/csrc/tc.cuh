@@ -16,6 +16,18 @@ enum : uint8_t { kClassNone = 0, kClassLight = 1, kClassSplit = 2, kClassCta = 3
 // Intersection variants a tile can run (the cost model's output order).
 enum : uint32_t { kVarHash = 0, kVarSearch = 1, kVarMerge = 2, kVarBitmap = 3 };
 
+// Can a warp run middle vertex v (d = d+(v), span = id span of N+(v)) with
+// variant `var`?  Sizes follow the warp's kWarpTableSlots shared words.
+__host__ __device__ __forceinline__ bool variant_legal(uint32_t var, uint32_t d, uint32_t span) {
+  switch (var) {
+    case kVarHash: return d <= kWarpTableSlots / 2;
+    case kVarSearch: return d <= kWarpTableSlots;
+    case kVarMerge: return d <= 8;
+    case kVarBitmap: return span <= (kWarpTableSlots - 1) * 32u - 1u;
+    default: return false;
+  }
+}
+
 // A unit of scheduled work over middle vertices v.
 //   j1 == kGroupTile : light vertices light[v0 .. v1) (the plan's compacted
 //                      list of light vertices), all their in-edges
@@ -82,10 +94,21 @@ struct gary_count_plan {
   uint32_t n_cta = 0;
   uint32_t n_warp = 0;
   gary::DevBuf<gary::SchedState> sched;
+  gary::DevBuf<uint8_t> variant;  // learned plans: intersection variant per middle vertex
+  bool learned = false;
 };
 
 namespace gary {
-int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_count_plan **out);
+// model: host copy of a cost-model parameter block (learned plan) or null
+int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_count_plan **out,
+                  const float *model = nullptr);
+// Cost-model features and legal-variant masks of every middle vertex.
+int k3_features(gary_graph *g, gary_count_plan *plan, float *d_x, uint8_t *d_legal, cudaStream_t s);
 int launch_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
               uint32_t shard, uint32_t nshards);
+// The same launch with a forced per-vertex variant array and/or a per-vertex
+// cycle log (profiling for the cost model).
+int launch_k3_ctl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
+                  uint32_t shard, uint32_t nshards, const uint8_t *variant,
+                  unsigned long long *cycles);
 }  // namespace gary

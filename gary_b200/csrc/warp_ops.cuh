@@ -73,6 +73,12 @@ __device__ __forceinline__ uint32_t warp_inclusive_sum(uint32_t x, int lane) {
   return x;
 }
 
+__device__ __forceinline__ float warp_sum_f32(float x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);

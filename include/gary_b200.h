@@ -236,6 +236,40 @@ int gary_gen_pairs_values(uint64_t seed, uint64_t first, uint64_t npairs, uint32
                           const uint32_t *d_la, const uint32_t *d_lb, const uint64_t *d_a_off,
                           const uint64_t *d_b_off, uint32_t *d_a, uint32_t *d_b, void *stream);
 
+/* ---- learned scheduling: the cost model ---------------------------------
+ * A 6 -> 64 -> 64 -> 4 MLP (FP32, ReLU) predicts, for every middle vertex of
+ * the triangle kernel, log2 of the cycles each intersection variant (hash,
+ * search, merge, bitmap: index 0..3) would take.  GARY_SCHED_LEARNED runs
+ * every warp vertex with its predicted-cheapest legal variant and cuts tiles
+ * by predicted cycles; the plain plan (bitmap when the id span fits, else
+ * hash; probe-count tile weights) stays the fallback.  No reference
+ * counterpart: the reference has one fixed variant per kernel.
+ *
+ * Parameter block of gary_mlp_param_count() floats: mu_x[6], sd_x[6],
+ * mu_y[4], sd_y[4] (standardisation), then W1[64][6], b1, W2[64][64], b2,
+ * W3[4][64], b3.  Training runs on the device: gary_mlp_grad (forward and
+ * backward, masked squared error in standardised units) and gary_mlp_adam.
+ * Files: "GARYMLP1", uint32 {1, 6, 64, 64, 4}, then the floats. */
+int gary_mlp_param_count(void);
+int gary_mlp_init(uint64_t seed, float *params);
+int gary_mlp_forward(const float *d_params, const float *d_x, uint64_t n, int scale, float *d_y,
+                     void *stream);
+int gary_mlp_grad(const float *d_params, const float *d_x, const float *d_t, const uint8_t *d_mask,
+                  uint64_t n, float norm, float *d_grad, float *d_loss, void *stream);
+int gary_mlp_adam(float *d_params, const float *d_grad, float *d_m, float *d_v, uint32_t step,
+                  float lr, void *stream);
+int gary_mlp_save(const char *path, const float *params);
+int gary_mlp_load(const char *path, float *params);
+/* Process-wide model for GARY_SCHED_LEARNED (host block; NULL clears). */
+int gary_set_cost_model(const float *params);
+/* Training data: features d_x[n][6] and legal-variant bits d_legal[n] of every
+ * middle vertex (0: not run by a warp), and per-vertex cycles of one run of
+ * the triangle kernel with every warp vertex forced to `variant` (-1: plain
+ * dispatch).  d_count receives the triangle count (exact for any variant). */
+int gary_tc_features(gary_graph *g, float *d_x, uint8_t *d_legal, void *stream);
+int gary_tc_profile(gary_graph *g, int variant, uint64_t *d_cycles, uint64_t *d_count,
+                    void *stream);
+
 /* ---- symmetric CSR construction on the device ------------------------- *
  * Dedup, drop self loops, symmetrise and sort an undirected edge list into a
  * CSR (the reference does this on the host: src/Graph.cpp:19-32, 63-91). */

@@ -283,3 +283,70 @@ int orc_binary_search_2phase(const uint32_t *list, int64_t n, const uint32_t *ca
   int64_t bottom = pos * n / N, top = (pos + 1) * n / N;
   return orc_binary_search(list + bottom, top - bottom, key);
 }
+
+/* ---- cost-model network (FP64) ------------------------------------------ */
+enum { NI = 6, NH1 = 64, NH2 = 64, NO = 4, OFF_W1 = 20, OFF_B1 = OFF_W1 + NH1 * NI,
+       OFF_W2 = OFF_B1 + NH1, OFF_B2 = OFF_W2 + NH2 * NH1, OFF_W3 = OFF_B2 + NH2,
+       OFF_B3 = OFF_W3 + NO * NH2, NPARAM = OFF_B3 + NO };
+
+static void mlp_fwd1(const float *P, const float *x, double *h1, double *h2, double *y) {
+  for (int i = 0; i < NH1; ++i) {
+    double a = P[OFF_B1 + i];
+    for (int f = 0; f < NI; ++f) a += (double)P[OFF_W1 + i * NI + f] * x[f];
+    h1[i] = a > 0 ? a : 0;
+  }
+  for (int j = 0; j < NH2; ++j) {
+    double a = P[OFF_B2 + j];
+    for (int i = 0; i < NH1; ++i) a += (double)P[OFF_W2 + j * NH1 + i] * h1[i];
+    h2[j] = a > 0 ? a : 0;
+  }
+  for (int k = 0; k < NO; ++k) {
+    double a = P[OFF_B3 + k];
+    for (int j = 0; j < NH2; ++j) a += (double)P[OFF_W3 + k * NH2 + j] * h2[j];
+    y[k] = a;
+  }
+}
+
+void orc_mlp_forward(const float *params, const float *x, int64_t n, double *y) {
+  double h1[NH1], h2[NH2];
+  for (int64_t s = 0; s < n; ++s) mlp_fwd1(params, x + s * NI, h1, h2, y + s * NO);
+}
+
+void orc_mlp_grad(const float *params, const float *x, const float *t, const uint8_t *mask,
+                  int64_t n, double norm, double *grad, double *loss) {
+  double h1[NH1], h2[NH2], y[NO], dy[NO], d2[NH2], d1[NH1];
+  memset(grad, 0, NPARAM * sizeof(double));
+  double L = 0;
+  for (int64_t s = 0; s < n; ++s) {
+    const float *xs = x + s * NI;
+    mlp_fwd1(params, xs, h1, h2, y);
+    for (int k = 0; k < NO; ++k) {
+      const double e = ((mask[s] >> k) & 1) ? y[k] - t[s * NO + k] : 0.0;
+      L += e * e;
+      dy[k] = 2.0 * e / norm;
+    }
+    for (int j = 0; j < NH2; ++j) {
+      double a = 0;
+      for (int k = 0; k < NO; ++k) a += (double)params[OFF_W3 + k * NH2 + j] * dy[k];
+      d2[j] = h2[j] > 0 ? a : 0;
+    }
+    for (int i = 0; i < NH1; ++i) {
+      double a = 0;
+      for (int j = 0; j < NH2; ++j) a += (double)params[OFF_W2 + j * NH1 + i] * d2[j];
+      d1[i] = h1[i] > 0 ? a : 0;
+    }
+    for (int k = 0; k < NO; ++k) {
+      for (int j = 0; j < NH2; ++j) grad[OFF_W3 + k * NH2 + j] += dy[k] * h2[j];
+      grad[OFF_B3 + k] += dy[k];
+    }
+    for (int j = 0; j < NH2; ++j) {
+      for (int i = 0; i < NH1; ++i) grad[OFF_W2 + j * NH1 + i] += d2[j] * h1[i];
+      grad[OFF_B2 + j] += d2[j];
+    }
+    for (int i = 0; i < NH1; ++i) {
+      for (int f = 0; f < NI; ++f) grad[OFF_W1 + i * NI + f] += d1[i] * xs[f];
+      grad[OFF_B1 + i] += d1[i];
+    }
+  }
+  *loss = L;
+}

@@ -66,6 +66,16 @@ void orc_build_cache(const uint32_t *list, int64_t n, int N, uint32_t *cache);
 int orc_binary_search_2phase(const uint32_t *list, int64_t n, const uint32_t *cache, int N,
                              uint32_t key);
 
+/* Cost-model network (6 -> 64 -> 64 -> 4, ReLU), FP64 restatement of the
+ * GPU kernels for gradient checks.  `params` uses the GPU block layout
+ * (20 normalisation floats, then W1, b1, W2, b2, W3, b3).  orc_mlp_grad
+ * returns d(loss)/d(weights) for loss = sum over masked cells of
+ * (y - t)^2 / norm, in standardised units, into grad[4888] (normalisation
+ * entries zero), and the unnormalised squared-error sum in *loss. */
+void orc_mlp_forward(const float *params, const float *x, int64_t n, double *y);
+void orc_mlp_grad(const float *params, const float *x, const float *t, const uint8_t *mask,
+                  int64_t n, double norm, double *grad, double *loss);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,8 @@ _ORC = {
     "orc_binary_search": (_INT, [_P, _I64, _U32]),
     "orc_build_cache": (None, [_P, _I64, _INT, _P]),
     "orc_binary_search_2phase": (_INT, [_P, _I64, _P, _INT, _U32]),
+    "orc_mlp_forward": (None, [_P, _P, _I64, _P]),
+    "orc_mlp_grad": (None, [_P, _P, _P, _P, _I64, C.c_double, _P, C.POINTER(C.c_double)]),
 }
 
 _REF_CPU = {
@@ -276,3 +278,19 @@ class RefGpuGraph:
             self.free()
         except Exception:
             pass
+
+
+def mlp_forward(params, x) -> np.ndarray:
+    params, x = _a(params, np.float32), _a(x, np.float32)
+    y = np.zeros((len(x), 4), np.float64)
+    orc().orc_mlp_forward(params.ctypes.data, x.ctypes.data, len(x), y.ctypes.data)
+    return y
+
+
+def mlp_grad(params, x, t, mask, norm: float):
+    params, x, t, mask = _a(params, np.float32), _a(x, np.float32), _a(t, np.float32), _a(mask, np.uint8)
+    g = np.zeros(len(params), np.float64)
+    loss = C.c_double()
+    orc().orc_mlp_grad(params.ctypes.data, x.ctypes.data, t.ctypes.data, mask.ctypes.data, len(x), norm,
+                       g.ctypes.data, C.byref(loss))
+    return g, loss.value

@@ -1,0 +1,144 @@
+"""The cost model: MLP kernels against the FP64 CPU restatement (gradients,
+forward pass, Adam), the file format, and exactness of every intersection
+variant and of the learned schedule."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import gary_b200 as gb
+from gary_b200 import _lib
+from gary_b200 import costmodel as cm
+from oracle import oracle as O
+
+P = None
+
+
+def _np_params(seed=3):
+    return cm.CostModel.init(seed).params
+
+
+def test_init_and_file_roundtrip(tmp_path):
+    a = cm.CostModel.init(7)
+    b = cm.CostModel.init(7)
+    assert np.array_equal(a.params, b.params)
+    assert a.params.size == 4888
+    path = tmp_path / "m.gmlp"
+    a.save(path)
+    c = cm.CostModel.load(path)
+    assert np.array_equal(a.params, c.params)
+    raw = path.read_bytes()
+    assert raw[:8] == b"GARYMLP1" and len(raw) == 8 + 20 + 4888 * 4
+    (tmp_path / "bad").write_bytes(b"NOTAMODEL" * 10)
+    with pytest.raises(gb.GaryError):
+        cm.CostModel.load(tmp_path / "bad")
+
+
+def _rand(n, seed):
+    r = np.random.default_rng(seed)
+    x = r.normal(size=(n, 6)).astype(np.float32)
+    t = r.normal(size=(n, 4)).astype(np.float32)
+    m = r.integers(0, 16, size=n).astype(np.uint8)
+    return x, t, m
+
+
+@pytest.mark.gpu
+def test_forward_matches_fp64(cuda):
+    import torch
+
+    p = _np_params(5)
+    x, _, _ = _rand(1000, 1)
+    y_ref = O.mlp_forward(p, x)
+    dp, dx = torch.from_numpy(p).cuda(), torch.from_numpy(x).cuda()
+    dy = torch.empty((1000, 4), dtype=torch.float32, device="cuda")
+    _lib.check(_lib.load().gary_mlp_forward(dp.data_ptr(), dx.data_ptr(), 1000, 0, dy.data_ptr(), None), "fwd")
+    assert np.allclose(dy.cpu().numpy(), y_ref, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 777])
+def test_gradient_matches_fp64(cuda, n):
+    """FP32 device gradient vs FP64 host gradient: relative error <= 1e-4 of
+    the largest component (accumulation order differs)."""
+    import torch
+
+    p = _np_params(11)
+    x, t, m = _rand(n, n)
+    norm = float(max(1, sum(bin(int(v)).count("1") for v in m)))
+    g_ref, loss_ref = O.mlp_grad(p, x, t, m, norm)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    dp, dx, dt, dm = dev(p), dev(x), dev(t), dev(m)
+    dg = torch.empty_like(dp)
+    dl = torch.zeros(1, dtype=torch.float32, device="cuda")
+    _lib.check(_lib.load().gary_mlp_grad(dp.data_ptr(), dx.data_ptr(), dt.data_ptr(), dm.data_ptr(), n, norm,
+                                         dg.data_ptr(), dl.data_ptr(), None), "grad")
+    g = dg.cpu().numpy().astype(np.float64)
+    scale = np.abs(g_ref).max()
+    assert np.abs(g - g_ref).max() <= 1e-4 * scale + 1e-7
+    assert np.all(g[:20] == 0)
+    assert abs(float(dl.item()) - loss_ref) <= 1e-4 * max(loss_ref, 1.0)
+    # and a central-difference check of an output-layer weight (the loss is
+    # quadratic in it, so the difference quotient is exact up to rounding)
+    w = 20 + 64 * 6 + 64 + 64 * 64 + 64 + 64 * 2 + 7
+    e = 1e-2
+    pp, pm = p.copy(), p.copy()
+    pp[w] += e
+    pm[w] -= e
+    _, lp = O.mlp_grad(pp, x, t, m, norm)
+    _, lm = O.mlp_grad(pm, x, t, m, norm)
+    fd = (lp - lm) / (2 * e) / norm
+    assert abs(fd - g_ref[w]) <= 1e-6 * max(abs(fd), 1e-3)
+
+
+@pytest.mark.gpu
+def test_adam_step_matches_numpy(cuda):
+    import torch
+
+    p = _np_params(2)
+    g = np.random.default_rng(0).normal(size=p.size).astype(np.float32)
+    dp = torch.from_numpy(p.copy()).cuda()
+    dg = torch.from_numpy(g).cuda()
+    m = torch.zeros_like(dp)
+    v = torch.zeros_like(dp)
+    for step in (1, 2):
+        _lib.check(_lib.load().gary_mlp_adam(dp.data_ptr(), dg.data_ptr(), m.data_ptr(), v.data_ptr(), step,
+                                             1e-2, None), "adam")
+    # numpy reference (weights only; the normalisation block is not trained)
+    pr, mr, vr = p.astype(np.float64), np.zeros(p.size), np.zeros(p.size)
+    for step in (1, 2):
+        mr = 0.9 * mr + 0.1 * g
+        vr = 0.999 * vr + 0.001 * g.astype(np.float64) ** 2
+        upd = 1e-2 * (mr / (1 - 0.9 ** step)) / (np.sqrt(vr / (1 - 0.999 ** step)) + 1e-8)
+        pr[20:] -= upd[20:]
+    assert np.allclose(dp.cpu().numpy(), pr, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_training_fits_a_known_function(cuda):
+    r = np.random.default_rng(4)
+    X = r.uniform(0, 10, size=(20000, 6)).astype(np.float32)
+    T = np.stack([X[:, 0] + 0.5 * X[:, 3], 2 * X[:, 1] - X[:, 2], np.abs(X[:, 4] - 5), X[:, 5] ** 0.5 * 3], 1)
+    T = T.astype(np.float32)
+    M = r.integers(1, 16, size=len(X)).astype(np.uint8)
+    model, stats = cm.train(X, T, M, epochs=25, batch=1024, lr=3e-3, log=None)
+    for name in cm.VARIANTS:
+        assert stats[f"val_r2_{name}"] > 0.97, stats
+
+
+@pytest.mark.gpu
+def test_every_variant_and_learned_schedule_are_exact(cuda):
+    """The four intersection variants, forced on every warp vertex, and the
+    learned schedule (any model) all give the plain count."""
+    src, dst = gb.gen_rmat(16, 8, 16 << 16)
+    ptr, idx = gb.csr_from_edges(src, dst, 1 << 16)
+    with gb.Graph.upload(ptr, idx, 1 << 16) as g:
+        want = g.count()
+        x, legal, cyc, cnt = cm.profile(g, variants=(-1, 0, 1, 2, 3))
+        assert cnt == want
+        assert x.shape == (1 << 16, 6) and legal.any()
+        assert (cyc[3] > 0).any() and (cyc[2] > 0).any()
+        for seed in (0, 1):
+            cm.CostModel.init(seed).install()
+            _lib.load().gary_graph_drop_plans(g.handle)
+            assert g.count(sched=_lib.GARY_SCHED_LEARNED) == want
+    _lib.load().gary_set_cost_model(None)
