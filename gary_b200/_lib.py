@@ -105,6 +105,12 @@ SIGNATURES = {
     "gary_count_last_stats": (_INT, [_P, C.POINTER(CountStats)]),
     "gary_count_triangles_noalloc": (_INT, [_P, _P, _P, _U32, _P, _P]),
     "gary_tune": (_INT, [C.c_char_p, _U64]),
+    "gary_batch_upload": (_INT, [_P, _U32, _P, _P, _U32, _U64, _U32, _P, C.POINTER(_P)]),
+    "gary_batch_count_async": (_INT, [_P, _INT, _P, _P, _P]),
+    "gary_batch_capture": (_INT, [_P, _INT, _P, _P, _P, C.POINTER(_P)]),
+    "gary_exec_launch": (_INT, [_P, _P]),
+    "gary_exec_free": (_INT, [_P]),
+    "gary_gen_ba": (_INT, [_U32, _U32, _U64, _P, _P, C.POINTER(_U64)]),
     "gary_mlp_param_count": (_INT, []),
     "gary_mlp_init": (_INT, [_U64, _P]),
     "gary_mlp_forward": (_INT, [_P, _P, _U64, _INT, _P, _P]),

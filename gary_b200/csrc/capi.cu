@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -52,7 +53,7 @@ int sm_count() {
 }
 
 int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
-           cudaStream_t s, gary_graph **out);
+           cudaStream_t s, gary_graph **out, const uint64_t *group_off, uint32_t ngroups);
 int build_coo(PaddedCSR &c, cudaStream_t s);
 int download(gary_graph *g, uint64_t *ptr, uint32_t *idx, uint32_t *perm, cudaStream_t s);
 
@@ -204,6 +205,79 @@ extern "C" int gary_tc_profile(gary_graph *g, int variant, uint64_t *d_cycles, u
   });
 }
 
+// ---- batches ------------------------------------------------------------
+struct gary_exec {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace gary {
+namespace {
+int batch_count(gary_graph *g, unsigned long long *d_counts, unsigned long long *d_total,
+                cudaStream_t s, int sched) {
+  GARY_CHECK_ARG(g != nullptr && d_counts != nullptr && d_total != nullptr, "NULL argument");
+  GARY_CHECK_ARG(g->ngroups > 0, "graph was not uploaded with gary_batch_upload");
+  const int slot = plan_slot(GARY_PATTERN_TRIANGLE, sched);
+  if (!g->plans[slot]) GARY_TRY(count_async(g, GARY_PATTERN_TRIANGLE, sched, s, d_total));
+  GARY_CUDA(cudaMemsetAsync(d_counts, 0, (uint64_t)g->ngroups * 8, s));
+  gary_count_plan *plan = g->plans[slot];
+  return launch_k3_ctl(g, plan, d_total, s, 0, 1, plan->variant.p, nullptr, d_counts);
+}
+}  // namespace
+}  // namespace gary
+
+extern "C" int gary_batch_count_async(gary_graph *g, int sched, uint64_t *d_counts, uint64_t *d_total,
+                                      void *stream) {
+  GARY_CHECK_ARG(sched == GARY_SCHED_PLAIN || sched == GARY_SCHED_LEARNED, "unknown scheduler");
+  return guarded("gary_batch_count_async", [&] {
+    return gary::batch_count(g, reinterpret_cast<unsigned long long *>(d_counts),
+                             reinterpret_cast<unsigned long long *>(d_total), gary::as_stream(stream),
+                             sched);
+  });
+}
+
+extern "C" int gary_batch_capture(gary_graph *g, int sched, uint64_t *d_counts, uint64_t *d_total,
+                                  void *stream, gary_exec **out) {
+  GARY_CHECK_ARG(out != nullptr, "out is NULL");
+  GARY_CHECK_ARG(stream != nullptr, "capture needs a non-default stream");
+  return guarded("gary_batch_capture", [&] {
+    cudaStream_t s = gary::as_stream(stream);
+    // plans are built (allocations, host syncs) before the capture begins
+    GARY_TRY(gary::batch_count(g, reinterpret_cast<unsigned long long *>(d_counts),
+                               reinterpret_cast<unsigned long long *>(d_total), s, sched));
+    GARY_CUDA(cudaStreamSynchronize(s));
+    auto e = std::make_unique<gary_exec>();
+    GARY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int st = gary::batch_count(g, reinterpret_cast<unsigned long long *>(d_counts),
+                                     reinterpret_cast<unsigned long long *>(d_total), s, sched);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (st != GARY_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    GARY_CUDA(ce);
+    e->graph = graph;
+    GARY_CUDA(cudaGraphInstantiate(&e->exec, graph, 0));
+    *out = e.release();
+    return GARY_OK;
+  });
+}
+
+extern "C" int gary_exec_launch(gary_exec *e, void *stream) {
+  GARY_CHECK_ARG(e != nullptr, "exec is NULL");
+  GARY_CUDA(cudaGraphLaunch(e->exec, gary::as_stream(stream)));
+  return GARY_OK;
+}
+
+extern "C" int gary_exec_free(gary_exec *e) {
+  if (!e) return GARY_OK;
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  delete e;
+  return GARY_OK;
+}
+
 extern "C" int gary_graph_drop_plans(gary_graph *g) {
   GARY_CHECK_ARG(g != nullptr, "graph is NULL");
   gary::free_plans(g);
@@ -217,7 +291,17 @@ extern "C" int gary_abi_version(void) { return GARY_ABI_VERSION; }
 extern "C" int gary_graph_upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n,
                                  uint64_t nnz, uint32_t flags, void *stream, gary_graph **out) {
   return guarded("gary_graph_upload", [&] {
-    return gary::upload(ptr, idx, n, nnz, flags, gary::as_stream(stream), out);
+    return gary::upload(ptr, idx, n, nnz, flags, gary::as_stream(stream), out, nullptr, 0);
+  });
+}
+
+extern "C" int gary_batch_upload(const uint64_t *group_off, uint32_t ngroups, const uint64_t *ptr,
+                                 const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
+                                 void *stream, gary_graph **out) {
+  GARY_CHECK_ARG(group_off != nullptr && ngroups >= 1, "need ngroups >= 1 and host group offsets");
+  GARY_CHECK_ARG(!(flags & GARY_KEEP_IDS), "GARY_KEEP_IDS is not supported for batches");
+  return guarded("gary_batch_upload", [&] {
+    return gary::upload(ptr, idx, n, nnz, flags, gary::as_stream(stream), out, group_off, ngroups);
   });
 }
 

@@ -103,3 +103,47 @@ extern "C" int gary_gen_er(uint32_t n, uint64_t m, uint64_t seed, uint32_t *src,
   }
   return GARY_OK;
 }
+
+// Barabasi-Albert: a K_{m+1} seed clique, then every new vertex attaches to m
+// distinct earlier vertices chosen with probability proportional to degree
+// (uniform draws from the list holding each vertex once per incident edge
+// end).  Counter-based draws keyed by (seed, draw index).  Writes the edges
+// (once each) and their number.
+extern "C" int gary_gen_ba(uint32_t n, uint32_t m, uint64_t seed, uint32_t *src, uint32_t *dst,
+                           uint64_t *count) {
+  GARY_CHECK_ARG(m >= 1 && n > m, "need 1 <= m < n");
+  GARY_CHECK_ARG(src && dst && count, "NULL argument");
+  const uint64_t key = gary::mix64(seed ^ 0x632BE59BD9B4E019ull);
+  std::vector<uint32_t> ends;
+  ends.reserve(2ull * ((uint64_t)m * (m + 1) / 2 + (uint64_t)(n - m - 1) * m));
+  uint64_t e = 0;
+  for (uint32_t a = 0; a <= m; ++a)
+    for (uint32_t b = a + 1; b <= m; ++b) {
+      src[e] = a;
+      dst[e] = b;
+      ++e;
+      ends.push_back(a);
+      ends.push_back(b);
+    }
+  uint64_t draw = 0;
+  std::vector<uint32_t> pick(m);
+  for (uint32_t v = m + 1; v < n; ++v) {
+    uint32_t got = 0;
+    while (got < m) {
+      const uint64_t r = gary::mix64(key + (draw++) * gary::kGolden);
+      const uint32_t t = ends[(size_t)(((r >> 32) * ends.size()) >> 32)];
+      bool dup = false;
+      for (uint32_t k = 0; k < got; ++k) dup |= pick[k] == t;
+      if (!dup) pick[got++] = t;
+    }
+    for (uint32_t k = 0; k < m; ++k) {
+      src[e] = v;
+      dst[e] = pick[k];
+      ++e;
+      ends.push_back(v);
+      ends.push_back(pick[k]);
+    }
+  }
+  *count = e;
+  return GARY_OK;
+}

@@ -266,6 +266,49 @@ int input_error(unsigned bits) {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// Stream compaction with 64-bit sizes (CUB DeviceSelect takes int64 counts;
+// arrays here exceed 2^31 entries for graphs of ~10^9 edges).
+namespace {
+struct NotAllOnes {
+  __host__ __device__ bool operator()(uint64_t k) const { return k != ~0ull; }
+};
+}  // namespace
+
+int compact_keys(DevBuf<uint64_t> &keys, uint64_t count, uint64_t &kept, cudaStream_t s) {
+  kept = 0;
+  if (!count) return GARY_OK;
+  DevBuf<uint64_t> out, nsel;
+  GARY_TRY(out.alloc(count, s));
+  GARY_TRY(nsel.alloc(1, s));
+  size_t tmp = 0;
+  GARY_CUDA(cub::DeviceSelect::If(nullptr, tmp, keys.p, out.p, nsel.p, (int64_t)count, NotAllOnes(), s));
+  DevBuf<uint8_t> t;
+  GARY_TRY(t.alloc(tmp, s));
+  GARY_CUDA(cub::DeviceSelect::If(t.p, tmp, keys.p, out.p, nsel.p, (int64_t)count, NotAllOnes(), s));
+  GARY_CUDA(cudaMemcpyAsync(&kept, nsel.p, 8, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  std::swap(keys, out);
+  return GARY_OK;
+}
+
+int unique_keys(DevBuf<uint64_t> &keys, uint64_t count, uint64_t &kept, cudaStream_t s) {
+  kept = 0;
+  if (!count) return GARY_OK;
+  DevBuf<uint64_t> out, nsel;
+  GARY_TRY(out.alloc(count, s));
+  GARY_TRY(nsel.alloc(1, s));
+  size_t tmp = 0;
+  GARY_CUDA(cub::DeviceSelect::Unique(nullptr, tmp, keys.p, out.p, nsel.p, (int64_t)count, s));
+  DevBuf<uint8_t> t;
+  GARY_TRY(t.alloc(tmp, s));
+  GARY_CUDA(cub::DeviceSelect::Unique(t.p, tmp, keys.p, out.p, nsel.p, (int64_t)count, s));
+  GARY_CUDA(cudaMemcpyAsync(&kept, nsel.p, 8, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  std::swap(keys, out);
+  return GARY_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Padded lists from sorted (row << lg | col) keys.
 int padded_from_keys(const DevBuf<uint64_t> &keys, uint64_t m, uint32_t n, int lg, PaddedCSR &c,
                      cudaStream_t s) {
@@ -311,7 +354,7 @@ int oriented_keys(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz, uin
     k_make_keys<<<grid_for(nnz), kThreads, 0, s>>>(rowid, didx, nnz, n, deg, rank, lg, dag,
                                                    validate, keys.p, err);
     GARY_CUDA(cudaGetLastError());
-    m = thrust::remove(pol, keys.p, keys.p + nnz, ~0ull) - keys.p;
+    GARY_TRY(compact_keys(keys, nnz, m, s));
   }
   DevBuf<uint64_t> alt;
   GARY_TRY(alt.alloc(std::max<uint64_t>(m, 1), s));
@@ -321,8 +364,40 @@ int oriented_keys(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz, uin
 
 // ---------------------------------------------------------------------------
 // Oriented upload.  Input CSR (symmetric or DAG) -> degree-oriented padded lists.
+namespace {
+// group id of caller vertex v: the g with off[g] <= v < off[g + 1]
+__global__ void k_group_ids(const uint64_t *__restrict__ off, uint32_t ngroups, uint32_t n,
+                            uint32_t *__restrict__ gid) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t b = 0, e = ngroups;  // last g with off[g] <= v
+    while (e - b > 1) {
+      const uint32_t m = (b + e) >> 1;
+      if (off[m] <= v) b = m;
+      else e = m;
+    }
+    gid[v] = b;
+  }
+}
+__global__ void k_rank_keys(const uint32_t *__restrict__ deg, const uint32_t *__restrict__ gid,
+                            uint32_t n, int degbits, uint64_t *__restrict__ key) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    key[v] = ((gid ? (uint64_t)gid[v] : 0ull) << degbits) | deg[v];
+}
+__global__ void k_gather_u32(const uint32_t *__restrict__ perm, const uint32_t *__restrict__ src,
+                             uint32_t n, uint32_t *__restrict__ dst) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    dst[i] = src[perm[i]];
+}
+}  // namespace
+
+// group_off (host, ngroups + 1 entries; may be null): vertices
+// [group_off[g], group_off[g+1]) form graph g of a disjoint union.  Ranks are
+// then taken within each graph, so every graph keeps a contiguous rank range.
 int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
-           cudaStream_t s, gary_graph **out) {
+           cudaStream_t s, gary_graph **out, const uint64_t *group_off, uint32_t ngroups) {
   const bool on_dev = flags & GARY_INPUT_DEVICE;
   const bool dag = flags & GARY_INPUT_DAG;
   const bool keep_ids = flags & GARY_KEEP_IDS;
@@ -377,27 +452,48 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   }
   g->max_degree = thrust::reduce(pol, deg.p, deg.p + n, 0u, MaxU32());
 
-  // 3. ranks by (degree, id): a stable radix sort of the ids on degree
-  DevBuf<uint32_t> rank;
+  // 3. ranks by (graph, degree, id): a stable radix sort of the ids
+  DevBuf<uint32_t> rank, gidc;
+  if (ngroups) {
+    GARY_CHECK_ARG(group_off[0] == 0 && group_off[ngroups] == n,
+                   "group offsets must start at 0 and end at n");
+    for (uint32_t k = 0; k < ngroups; ++k)
+      GARY_CHECK_ARG(group_off[k] <= group_off[k + 1], "group offsets must be non-decreasing");
+    g->group_off.assign(group_off, group_off + ngroups + 1);
+    DevBuf<uint64_t> doff;
+    GARY_TRY(doff.alloc((uint64_t)ngroups + 1, s));
+    GARY_CUDA(cudaMemcpyAsync(doff.p, group_off, ((uint64_t)ngroups + 1) * 8, cudaMemcpyHostToDevice, s));
+    GARY_TRY(gidc.alloc(n, s));
+    k_group_ids<<<grid_for(n), kThreads, 0, s>>>(doff.p, ngroups, n, gidc.p);
+    GARY_CUDA(cudaGetLastError());
+  }
   {
-    DevBuf<uint32_t> dk, dk2, perm2;
+    const int degbits = bits_for((uint64_t)g->max_degree + 1);
+    const int keybits = degbits + (ngroups ? bits_for(ngroups) : 0);
+    DevBuf<uint64_t> dk, dk2;
+    DevBuf<uint32_t> perm2;
     GARY_TRY(dk.alloc(n, s));
     GARY_TRY(dk2.alloc(n, s));
     GARY_TRY(g->perm.alloc_persistent(n));
     GARY_TRY(perm2.alloc_persistent(n));
-    GARY_CUDA(cudaMemcpyAsync(dk.p, deg.p, (uint64_t)n * 4, cudaMemcpyDeviceToDevice, s));
+    k_rank_keys<<<grid_for(n), kThreads, 0, s>>>(deg.p, ngroups ? gidc.p : nullptr, n, degbits, dk.p);
     thrust::sequence(pol, perm2.p, perm2.p + n, 0u);
-    cub::DoubleBuffer<uint32_t> kb(dk.p, dk2.p), vb(perm2.p, g->perm.p);
+    cub::DoubleBuffer<uint64_t> kb(dk.p, dk2.p);
+    cub::DoubleBuffer<uint32_t> vb(perm2.p, g->perm.p);
     size_t tmp = 0;
-    int eb = bits_for((uint64_t)g->max_degree + 1);
-    GARY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kb, vb, n, 0, eb, s));
+    GARY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kb, vb, n, 0, keybits, s));
     DevBuf<uint8_t> t;
     GARY_TRY(t.alloc(tmp, s));
-    GARY_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kb, vb, n, 0, eb, s));
+    GARY_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kb, vb, n, 0, keybits, s));
     if (vb.Current() != g->perm.p) std::swap(g->perm, perm2);
     GARY_TRY(rank.alloc(n, s));
     GARY_TRY(g->rdeg.alloc_persistent(n));
     k_rank_scatter<<<grid_for(n), kThreads, 0, s>>>(g->perm.p, deg.p, n, rank.p, g->rdeg.p);
+    if (ngroups) {
+      g->ngroups = ngroups;
+      GARY_TRY(g->gid.alloc_persistent(n));
+      k_gather_u32<<<grid_for(n), kThreads, 0, s>>>(g->perm.p, gidc.p, n, g->gid.p);
+    }
     GARY_CUDA(cudaGetLastError());
   }
 
@@ -514,7 +610,7 @@ int csr_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_
   if (m) {
     k_edge_keys<<<grid_for(m), kThreads, 0, s>>>(src, dst, m, n, lg, keys.p, err.p);
     GARY_CUDA(cudaGetLastError());
-    k = thrust::remove(pol, keys.p, keys.p + 2 * m, ~0ull) - keys.p;
+    GARY_TRY(compact_keys(keys, 2 * m, k, s));
   }
   s_own.release();
   d_own.release();
@@ -524,7 +620,7 @@ int csr_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_
   GARY_TRY(alt.alloc(std::max<uint64_t>(k, 1), s));
   if (k) {
     GARY_TRY(radix_sort_keys(keys, alt, k, 2 * lg, s));
-    k = thrust::unique(pol, keys.p, keys.p + k) - keys.p;
+    GARY_TRY(unique_keys(keys, k, k, s));
   }
   alt.release();
   DevBuf<uint64_t> rowstart;
@@ -586,11 +682,20 @@ int build_coo(PaddedCSR &c, cudaStream_t s) {
   auto pol = thrust::cuda::par_nosync.on(s);
   DevBuf<uint32_t> rowid;
   GARY_TRY(padded_rowid(c, rowid, s));
-  DevBuf<uint64_t> words;
+  DevBuf<uint64_t> words, nsel;
   GARY_TRY(words.alloc(c.m, s));
-  uint64_t got = thrust::copy_if(pol, thrust::counting_iterator<uint64_t>(0),
-                                 thrust::counting_iterator<uint64_t>(c.words), words.p,
-                                 IsReal{c.adj.p}) - words.p;
+  GARY_TRY(nsel.alloc(1, s));
+  uint64_t got = 0;
+  {
+    cub::CountingInputIterator<uint64_t> it(0);
+    size_t tmp = 0;
+    GARY_CUDA(cub::DeviceSelect::If(nullptr, tmp, it, words.p, nsel.p, (int64_t)c.words, IsReal{c.adj.p}, s));
+    DevBuf<uint8_t> t;
+    GARY_TRY(t.alloc(tmp, s));
+    GARY_CUDA(cub::DeviceSelect::If(t.p, tmp, it, words.p, nsel.p, (int64_t)c.words, IsReal{c.adj.p}, s));
+    GARY_CUDA(cudaMemcpyAsync(&got, nsel.p, 8, cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaStreamSynchronize(s));
+  }
   if (got != c.m) {
     set_error("internal: padded adjacency holds %llu ids, expected %llu",
               (unsigned long long)got, (unsigned long long)c.m);
@@ -641,7 +746,7 @@ int build_symmetric(gary_graph *g, cudaStream_t s) {
     GARY_TRY(keys.alloc(std::max<uint64_t>(2 * W, 1), s));
     if (W) k_sym_keys<<<grid_for(W), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, rowid.p, W, lg, keys.p);
     GARY_CUDA(cudaGetLastError());
-    m2 = thrust::remove(pol, keys.p, keys.p + 2 * W, ~0ull) - keys.p;
+    GARY_TRY(compact_keys(keys, 2 * W, m2, s));
   }
   {
     DevBuf<uint64_t> alt;

@@ -57,6 +57,10 @@ struct gary_graph {
   gary::DevBuf<uint64_t> wedge;  // per vertex: sum of d+(w) over w in N+(v)
   gary::DevBuf<uint32_t> perm;   // rank -> caller id
   gary::DevBuf<uint32_t> rdeg;   // undirected degree by rank id (cost-model feature)
+  // disjoint union of several graphs (gary_batch_upload): graph of each rank id
+  uint32_t ngroups = 0;
+  std::vector<uint64_t> group_off;
+  gary::DevBuf<uint32_t> gid;
 
   // symmetric ranked lists (built lazily for 4-cycle counting)
   gary::PaddedCSR sym;
@@ -72,7 +76,8 @@ struct gary_graph {
   gary::GraphView view() const { return gary::GraphView{n, dag.row.p, dag.adj.p, true}; }
   gary::PaddedCSR &user_view() { return keep_ids ? kept : dag; }
   uint64_t device_bytes() const {
-    return dag.bytes() + kept.bytes() + sym.bytes() + wedge.bytes() + perm.bytes() + rdeg.bytes();
+    return dag.bytes() + kept.bytes() + sym.bytes() + wedge.bytes() + perm.bytes() + rdeg.bytes() +
+           gid.bytes();
   }
 };
 

@@ -90,6 +90,18 @@ __global__ void k_in_candidates(const uint2 *__restrict__ row, const uint32_t *_
   }
 }
 
+// first index i with keys[i] >= x in a sorted array (one thread)
+__global__ void k_first_geq(const uint32_t *__restrict__ keys, uint64_t len, uint32_t x,
+                            uint64_t *__restrict__ out) {
+  uint64_t b = 0, e = len;
+  while (b < e) {
+    const uint64_t m = (b + e) >> 1;
+    if (keys[m] < x) b = m + 1;
+    else e = m;
+  }
+  *out = b;
+}
+
 __global__ void k_in_heads(const uint32_t *__restrict__ keys, uint64_t m,
                            uint64_t *__restrict__ inptr) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
@@ -323,7 +335,15 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
   keys2.release();
   vals2.release();
   // records = number of keys < n (the rest carry the "no record" key n)
-  const uint64_t m = thrust::lower_bound(pol, keys.p, keys.p + W, n) - keys.p;
+  uint64_t m = 0;
+  {
+    DevBuf<uint64_t> pos;
+    GARY_TRY(pos.alloc(1, s));
+    k_first_geq<<<1, 1, 0, s>>>(keys.p, W, n, pos.p);
+    GARY_CUDA(cudaGetLastError());
+    GARY_CUDA(cudaMemcpyAsync(&m, pos.p, 8, cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaStreamSynchronize(s));
+  }
   in.records = m;
   GARY_TRY(in.inptr.alloc_persistent((uint64_t)n + 1));
   thrust::fill(pol, in.inptr.p, in.inptr.p + n + 1, m);
@@ -543,7 +563,8 @@ __device__ __forceinline__ uint32_t cta_walk(const uint4 *__restrict__ adj4,
 template <int WARPS>
 __device__ uint32_t cta_tile(const GraphView &g, const uint2 *__restrict__ inedge,
                              const uint64_t *__restrict__ inptr, const Tile &t, uint32_t *smem,
-                             uint32_t *chunk, uint64_t *bar, uint32_t &phase, unsigned *err) {
+                             uint32_t *chunk, uint64_t *bar, uint32_t &phase, unsigned *err,
+                             const uint32_t *gid, unsigned long long *gcount) {
   constexpr uint32_t S = WARPS * kWarpTableSlots;  // shared words
   const int lane = threadIdx.x & 31;
   const uint32_t v = t.v0;
@@ -579,6 +600,10 @@ __device__ uint32_t cta_tile(const GraphView &g, const uint2 *__restrict__ inedg
     }
     const SearchSet st{av, smem, d, S, lo, span};
     cnt = cta_walk<WARPS>(adj4, inedge, kb, ke, chunk, lane, st);
+  }
+  if (gcount) {
+    const unsigned long long tw = warp_sum_u64(cnt);
+    if (lane == 0 && tw) atomicAdd(&gcount[gid[v]], tw);
   }
   // the next tile rewrites shared memory, possibly through the async proxy
   fence_proxy_async_smem();
@@ -621,7 +646,17 @@ struct RegSet8 {
 struct VertexCtl {
   const uint8_t *variant;      // intersection variant per middle vertex
   unsigned long long *cycles;  // clock64 cycles spent per middle vertex
+  const uint32_t *gid;         // batches: graph of each middle vertex
+  unsigned long long *gcount;  // batches: per-graph counts
 };
+
+// Batches: add a warp's count for middle vertex v to its graph's total.
+__device__ __forceinline__ void add_graph_count(const VertexCtl &ctl, uint32_t v, uint32_t c,
+                                                int lane) {
+  if (!ctl.gcount) return;
+  const unsigned long long t = warp_sum_u64(c);
+  if (lane == 0 && t) atomicAdd(&ctl.gcount[ctl.gid[v]], t);
+}
 
 // One middle vertex v on one warp: a set of N+(v) in the warp's slots, walk
 // in-edges [j0, j1) of v.
@@ -666,6 +701,7 @@ __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 
   }
   __syncwarp();
   if (ctl.cycles && lane == 0) atomicAdd(&ctl.cycles[v], (unsigned long long)(clock64() - t0));
+  add_graph_count(ctl, v, c, lane);
   return c;
 }
 
@@ -695,7 +731,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     __syncthreads();
     if (t >= rng.cta_hi) break;
     const Tile tl = tiles[t];
-    cnt += cta_tile<WARPS>(g, inedge, inptr, tl, smem, &s_chunk, &bar, phase, &sched->error);
+    cnt += cta_tile<WARPS>(g, inedge, inptr, tl, smem, &s_chunk, &bar, phase, &sched->error,
+                           ctl.gid, ctl.gcount);
   }
 
   // phase 2: warp tiles, each warp on its own slots
@@ -753,31 +790,34 @@ int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_o
   if (per_sm < 1) per_sm = 1;
   const unsigned grid = (unsigned)(sm_count() * per_sm);
   const TileRange rng = shard_range(plan->n_cta, plan->n_warp, shard, nshards);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  GARY_CUDA(cudaStreamIsCapturing(s, &cap));
+  const bool timed = cap == cudaStreamCaptureStatusNone;
   GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
   GARY_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), s));
-  GARY_CUDA(cudaEventRecord(g->ev0, s));
+  if (timed) GARY_CUDA(cudaEventRecord(g->ev0, s));
   kern<<<grid, WARPS * 32, smem, s>>>(g->view(), plan->in.inedge.p, plan->in.inptr.p, plan->light.p,
                                       plan->tiles.p, plan->n_cta, rng, plan->sched.p, d_out, ctl);
   GARY_CUDA(cudaGetLastError());
-  GARY_CUDA(cudaEventRecord(g->ev1, s));
+  if (timed) GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
   g->last.tiles = (rng.cta_hi - rng.cta_lo) + (rng.warp_hi - rng.warp_lo);
   g->last.cta_tiles = rng.cta_hi - rng.cta_lo;
-  g->last_timed = true;
+  g->last_timed = timed;
   return GARY_OK;
 }
 
 int launch_k3_ctl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
                   uint32_t shard, uint32_t nshards, const uint8_t *variant,
-                  unsigned long long *cycles) {
-  const VertexCtl ctl{variant, cycles};
+                  unsigned long long *cycles, unsigned long long *gcount) {
+  const VertexCtl ctl{variant, cycles, gcount ? g->gid.p : nullptr, gcount};
   if (plan->params.min_blocks >= 3) return launch_k3_impl<3>(g, plan, d_out, s, shard, nshards, ctl);
   return launch_k3_impl<2>(g, plan, d_out, s, shard, nshards, ctl);
 }
 
 int launch_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
               uint32_t shard, uint32_t nshards) {
-  return launch_k3_ctl(g, plan, d_out, s, shard, nshards, plan->variant.p, nullptr);
+  return launch_k3_ctl(g, plan, d_out, s, shard, nshards, plan->variant.p, nullptr, nullptr);
 }
 
 }  // namespace gary

@@ -110,5 +110,5 @@ int launch_k3(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, c
 // cycle log (profiling for the cost model).
 int launch_k3_ctl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
                   uint32_t shard, uint32_t nshards, const uint8_t *variant,
-                  unsigned long long *cycles);
+                  unsigned long long *cycles, unsigned long long *gcount = nullptr);
 }  // namespace gary

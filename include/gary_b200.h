@@ -175,6 +175,33 @@ int gary_count_triangles_noalloc(const uint64_t *d_indptr, const uint32_t *d_col
                                  const uint32_t *d_deg, uint32_t n, void *stream,
                                  uint64_t *d_out);
 
+/* ---- batches of graphs ---------------------------------------------------
+ * Many graphs counted in one persistent launch.  gary_batch_upload takes the
+ * disjoint union as one CSR whose vertices [group_off[g], group_off[g+1])
+ * form graph g (host offsets, ngroups + 1 entries) and ranks vertices within
+ * each graph.  gary_batch_count_async writes the triangle count of every
+ * graph to d_counts[g] and their sum to *d_total; the work of all graphs is
+ * cut into one tile list fed to the kernel by its device-side queue.
+ * gary_batch_capture records that count (queue reset, zeroing, kernel) into a
+ * CUDA graph; gary_exec_launch replays it.  No reference counterpart: the
+ * reference counts one graph per launch (test/TriQueryTest.cu:114-133). */
+typedef struct gary_exec gary_exec;
+int gary_batch_upload(const uint64_t *group_off, uint32_t ngroups, const uint64_t *ptr,
+                      const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags, void *stream,
+                      gary_graph **out);
+int gary_batch_count_async(gary_graph *g, int sched, uint64_t *d_counts, uint64_t *d_total,
+                           void *stream);
+int gary_batch_capture(gary_graph *g, int sched, uint64_t *d_counts, uint64_t *d_total,
+                       void *stream, gary_exec **out);
+int gary_exec_launch(gary_exec *e, void *stream);
+int gary_exec_free(gary_exec *e);
+
+/* Barabasi-Albert graph (seed clique K_{m+1}, m distinct degree-proportional
+ * targets per new vertex); edges written once each, *count receives their
+ * number (<= m (m+1) / 2 + (n - m - 1) m). */
+int gary_gen_ba(uint32_t n, uint32_t m, uint64_t seed, uint32_t *src, uint32_t *dst,
+                uint64_t *count);
+
 /* ---- tuning (the autotuner's knobs) -------------------------------------
  * Process-wide parameters of the counting plans, applied to plans built after
  * the call (gary_graph_drop_plans discards a graph's cached plans):
