@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--sched", choices=["plain", "learned"], default="plain")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--pool-keep-gb", type=float, default=None,
+                    help="freed construction scratch the library's memory pool keeps mapped (GB)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU sample time")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference GPU kernel")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -254,6 +256,8 @@ def run_ours(args, dist):
 
     dist.init(torch)
     dev = dist.local
+    if args.pool_keep_gb is not None:
+        _lib.check(_lib.load().gary_tune(b"pool_keep_bytes", int(args.pool_keep_gb * 1e9)), "gary_tune")
     sched = {"plain": _lib.GARY_SCHED_PLAIN, "learned": _lib.GARY_SCHED_LEARNED}[args.sched]
     t_build = time.perf_counter()
     n, csr = build_graph(gb, torch, args.scale, args.ef, args.seed)
@@ -366,7 +370,12 @@ def run_ours(args, dist):
             "count": count,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
-                         "alg_bytes_per_launch": alg / dist.world},
+                         "alg_bytes_per_launch": alg / dist.world,
+                         # DRAM bytes one launch moved (ncu, same workload) over its live duration:
+                         # the middle-vertex walk serves most list reads from L2, so this sits
+                         # far below the algorithmic figure
+                         "dram_gbs": traffic / (ms_local / 1e3) / 1e9 if traffic else None,
+                         "dram_frac": traffic / (ms_local / 1e3) / 1e9 / hbm if traffic else None},
             "e2e": e2e,
             "gpu_launches": args.steps,
             "clocks": clk,

@@ -2,8 +2,10 @@
 // No C++ exception crosses this boundary: every entry point catches and maps
 // to a GARY_ERR_* status (the reference's checkCudaErrors exits the process
 // instead, common/HelperCUDA.h:582-595).
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -50,6 +52,79 @@ int sm_count() {
   }
   if (d >= 0 && d < 64) cache[d] = v;
   return v;
+}
+
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+uint64_t g_pool_keep = ~0ull;  // keep freed scratch mapped, as a caching allocator does
+}  // namespace
+
+cudaMemPool_t scratch_pool() {
+  const int d = device_ordinal();
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (d < 0 || d >= 64) {
+    cudaMemPool_t p = nullptr;
+    cudaDeviceGetDefaultMemPool(&p, d);
+    return p;
+  }
+  if (!g_pools[d]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = d;
+    if (cudaMemPoolCreate(&g_pools[d], &props) != cudaSuccess) {
+      cudaGetLastError();
+      cudaDeviceGetDefaultMemPool(&g_pools[d], d);
+    } else {
+      uint64_t keep = g_pool_keep;
+      cudaMemPoolSetAttribute(g_pools[d], cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
+  return g_pools[d];
+}
+
+void set_pool_keep_bytes(uint64_t bytes) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  g_pool_keep = bytes;
+  for (cudaMemPool_t p : g_pools) {
+    if (!p) continue;
+    uint64_t keep = bytes;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaMemPoolTrimTo(p, bytes);
+  }
+}
+
+namespace {
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+bool trace_on() {
+  static const bool on = [] {
+    const char *e = std::getenv("GARY_TRACE");
+    return e && *e && std::strcmp(e, "0") != 0;
+  }();
+  return on;
+}
+}  // namespace
+
+PhaseTrace::PhaseTrace(const char *what_, cudaStream_t s_) : what(what_), s(s_), on(trace_on()) {
+  if (on) {
+    cudaStreamSynchronize(s);
+    t0 = t = now_s();
+  }
+}
+
+void PhaseTrace::mark(const char *phase) {
+  if (!on) return;
+  cudaStreamSynchronize(s);
+  const double x = now_s();
+  std::fprintf(stderr, "[gary trace] %s: %-24s %9.3f ms\n", what, phase, (x - t) * 1e3);
+  t = x;
+}
+
+PhaseTrace::~PhaseTrace() {
+  if (on) std::fprintf(stderr, "[gary trace] %s: %-24s %9.3f ms\n", what, "total", (now_s() - t0) * 1e3);
 }
 
 int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
@@ -156,6 +231,7 @@ extern "C" int gary_tune(const char *key, uint64_t value) {
   else if (k == "cta_tile_cost" && value > 0) p.cta_tile_cost = value;
   else if (k == "vertex_overhead") p.vertex_overhead = value;
   else if (k == "min_blocks" && (value == 2 || value == 3)) p.min_blocks = (uint32_t)value;
+  else if (k == "pool_keep_bytes") gary::set_pool_keep_bytes(value);
   else if (k == "reset") p = gary::PlanParams{};
   else {
     gary::set_error("unknown tuning key '%s' or value %llu out of range", key,

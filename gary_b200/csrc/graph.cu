@@ -417,6 +417,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   g->flags = flags;
   g->keep_ids = keep_ids;
   auto pol = thrust::cuda::par_nosync.on(s);
+  PhaseTrace tr("upload", s);
 
   // 1. input on the device
   DevBuf<uint64_t> dptr_own;
@@ -433,6 +434,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
     didx = didx_own.p;
   }
 
+  tr.mark("h2d input");
   DevBuf<unsigned> err;
   GARY_TRY(err.alloc(1, s));
   GARY_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), s));
@@ -452,6 +454,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   }
   g->max_degree = thrust::reduce(pol, deg.p, deg.p + n, 0u, MaxU32());
 
+  tr.mark("degrees");
   // 3. ranks by (graph, degree, id): a stable radix sort of the ids
   DevBuf<uint32_t> rank, gidc;
   if (ngroups) {
@@ -497,6 +500,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
     GARY_CUDA(cudaGetLastError());
   }
 
+  tr.mark("ranks");
   // 4. row id of every entry: heads, then an inclusive max-scan
   const int lg = bits_for(n);
   DevBuf<uint32_t> rowid;
@@ -511,6 +515,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
     GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
   }
 
+  tr.mark("row ids");
   // 5. oriented, ranked keys: sorted, validated
   DevBuf<uint64_t> keys;
   uint64_t m = 0;
@@ -525,8 +530,10 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
     if (herr) return input_error(herr);
   }
 
+  tr.mark("oriented keys + sort");
   // 6. the kernels' padded lists, per-vertex wedge counts, statistics
   GARY_TRY(padded_from_keys(keys, m, n, lg, g->dag, s));
+  tr.mark("padded lists");
   GARY_TRY(g->wedge.alloc_persistent(n));
   GARY_CUDA(cudaMemsetAsync(g->wedge.p, 0, (uint64_t)n * 8, s));
   if (m)
@@ -538,6 +545,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   g->wedges = thrust::reduce(pol, g->wedge.p, g->wedge.p + n, 0ull);
   g->alg_bytes = 4 * g->out_deg_sq + 4 * g->wedges + 24 * m;
   keys.release();
+  tr.mark("wedges + statistics");
 
   // 7. the same orientation in caller ids, for the views (GARY_KEEP_IDS)
   if (keep_ids) {

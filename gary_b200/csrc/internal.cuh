@@ -43,10 +43,34 @@ void clear_error();
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// ---- stream-ordered scratch pool -----------------------------------------
+// One cudaMemPool per device, owned by the library, for the temporaries of
+// graph construction and plan building.  Its release threshold (tuning key
+// "pool_keep_bytes") is how much freed scratch the pool keeps mapped across
+// synchronisations.  The default keeps all of it (a caching allocator: the
+// next upload reuses the mapped pages); 0 hands everything back to the
+// driver at each sync, and the next upload then pays to map its pages again
+// (about 7x the upload time at 10^9 edges).
+cudaMemPool_t scratch_pool();
+void set_pool_keep_bytes(uint64_t bytes);
+
+// ---- phase trace (GARY_TRACE=1 in the environment) -----------------------
+// mark() synchronises the stream and prints the wall time since the previous
+// mark to stderr; with tracing off it does nothing and costs nothing.
+struct PhaseTrace {
+  const char *what;
+  cudaStream_t s;
+  bool on;
+  double t0, t;
+  PhaseTrace(const char *what, cudaStream_t s);
+  void mark(const char *phase);
+  ~PhaseTrace();
+};
+
 // ---- device buffer with RAII --------------------------------------------
-// alloc(): stream-ordered temporary (cudaMallocAsync / cudaFreeAsync on the
-// same stream).  alloc_persistent(): cudaMalloc / cudaFree, for arrays that
-// outlive the call and so must not depend on the caller's stream.
+// alloc(): stream-ordered temporary from the scratch pool (freed on the same
+// stream).  alloc_persistent(): cudaMalloc / cudaFree, for arrays that outlive
+// the call and so must not depend on the caller's stream.
 template <typename T>
 struct DevBuf {
   T *p = nullptr;
@@ -86,7 +110,8 @@ struct DevBuf {
     n = count;
     if (count == 0) return GARY_OK;
     cudaError_t e = is_async
-        ? cudaMallocAsync(reinterpret_cast<void **>(&p), count * sizeof(T), stream)
+        ? cudaMallocFromPoolAsync(reinterpret_cast<void **>(&p), count * sizeof(T),
+                                  scratch_pool(), stream)
         : cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;

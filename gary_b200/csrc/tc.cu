@@ -371,7 +371,9 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
   plan->params = pp;
   const uint32_t n = g->n;
   auto pol = thrust::cuda::par_nosync.on(s);
+  PhaseTrace tr("triangle plan", s);
   GARY_TRY(build_in_index(g, s, plan->in));
+  tr.mark("in-edge index");
   GARY_TRY(plan->vclass.alloc_persistent(n));
   DevBuf<uint64_t> costV;  // cost of each light vertex, 0 for the others
   DevBuf<uint32_t> kW, kC;
@@ -413,6 +415,7 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
   GARY_CUDA(cudaMemcpyAsync(&nW, kW.p + n, 4, cudaMemcpyDeviceToHost, s));
   GARY_CUDA(cudaMemcpyAsync(&nC, kC.p + n, 4, cudaMemcpyDeviceToHost, s));
   GARY_CUDA(cudaStreamSynchronize(s));
+  tr.mark("classify");
   const uint64_t G = totalL ? (totalL + tw - 1) / tw : 0;
   const uint64_t total = (uint64_t)nC + nW + G;
   if (total >= (1ull << 31)) {
@@ -448,6 +451,7 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
   }
   GARY_TRY(plan->sched.alloc_persistent(1));
   GARY_CUDA(cudaStreamSynchronize(s));
+  tr.mark("tiles");
   *out = plan.release();
   return GARY_OK;
 }

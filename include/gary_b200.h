@@ -209,7 +209,12 @@ int gary_gen_ba(uint32_t n, uint32_t m, uint64_t seed, uint32_t *src, uint32_t *
  *   "cta_tile_cost"   target probes per CTA tile         (default 2^20)
  *   "vertex_overhead" fixed cost charged per vertex      (default 64)
  *   "min_blocks"      resident CTAs per SM, 2 or 3       (default 2)
- *   "reset"           restore every default
+ *   "pool_keep_bytes" freed construction scratch the library's per-device
+ *                     memory pool keeps mapped across syncs (default
+ *                     UINT64_MAX: all of it, like a caching allocator; 0
+ *                     trims the pool now and hands scratch back at every
+ *                     sync); "reset" leaves it alone
+ *   "reset"           restore every plan default
  * No reference counterpart: the reference fixes its launch shape in each test
  * (test/TriQueryTest.cu:98-99, 116-117). */
 int gary_tune(const char *key, uint64_t value);
