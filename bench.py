@@ -65,41 +65,6 @@ def parse():
 
 
 # ---------------------------------------------------------------- plumbing
-class Dist:
-    def __init__(self):
-        self.world = int(os.environ.get("WORLD_SIZE", "1"))
-        self.rank = int(os.environ.get("RANK", "0"))
-        self.local = int(os.environ.get("LOCAL_RANK", "0"))
-        self.pg = None
-
-    def init(self, torch):
-        torch.cuda.set_device(self.local)
-        if self.world > 1:
-            import datetime
-
-            import torch.distributed as dist
-
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local))
-            self.pg = dist
-
-    def barrier(self):
-        if self.pg:
-            self.pg.barrier()
-
-    def allreduce(self, torch, x: float | int, op: str):
-        if not self.pg:
-            return x
-        dt = torch.float64 if isinstance(x, float) else torch.int64
-        t = torch.tensor([x], dtype=dt, device="cuda")
-        self.pg.all_reduce(t, op={"max": self.pg.ReduceOp.MAX, "sum": self.pg.ReduceOp.SUM}[op])
-        return t.item()
-
-    def close(self):
-        if self.pg:
-            self.pg.destroy_process_group()
-
-
 class Clocks:
     """nvidia-smi sampler running during the timed region."""
 
@@ -254,7 +219,7 @@ def run_ours(args, dist):
     import gary_b200 as gb
     from gary_b200 import _lib
 
-    dist.init(torch)
+    dist.init()
     dev = dist.local
     if args.pool_keep_gb is not None:
         _lib.check(_lib.load().gary_tune(b"pool_keep_bytes", int(args.pool_keep_gb * 1e9)), "gary_tune")
@@ -298,8 +263,8 @@ def run_ours(args, dist):
     clk = clocks.stop()
     per = [a.elapsed_time(b) for a, b in evs]
     ms_local = sum(per) / len(per)
-    ms = dist.allreduce(torch, ms_local, "max")
-    count = dist.allreduce(torch, count_local, "sum")
+    ms = dist.allreduce(ms_local, "max")
+    count = dist.allreduce(count_local, "sum")
     value = m / (ms / 1e3)
 
     # ---- end to end through the public API from pinned host memory
@@ -333,7 +298,7 @@ def run_ours(args, dist):
             if k > 0:  # first one warms the allocator
                 e2e_times.append(dt)
             assert res.value == count_local, "e2e count differs from the resident-graph count"
-        e2e_s = dist.allreduce(torch, sum(e2e_times) / len(e2e_times), "max")
+        e2e_s = dist.allreduce(sum(e2e_times) / len(e2e_times), "max")
         e2e = {"value": m / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (n + 1) * 8 + sym_nnz * 4,
                "d2h_bytes_per_step": 8, "ms_per_step": e2e_s * 1e3,
                "path": "gary_graph_upload(pinned host symmetric CSR) + gary_count_shard_async + D2H of the count"}
@@ -583,8 +548,10 @@ def load_lib():
 
 
 def main():
+    from gary_b200.dist import Dist
+
     args = parse()
-    dist = Dist()
+    dist = Dist.from_env()
     if args.workload == "setops":
         return run_setops(args, dist)
     if args.workload == "batch":

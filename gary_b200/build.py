@@ -101,11 +101,27 @@ def build_oracle(verbose: bool = False) -> None:
         print(r.stdout)
 
 
+def build_shim_tests(verbose: bool = False) -> None:
+    """Compile the C++ shim test programs (tests/cpp) against the built library."""
+    d = ROOT / "tests" / "cpp"
+    if not (d / "Makefile").exists():
+        return
+    cmd = ["make", "-s", "-C", str(d), f"NVCC={nvcc()}", "all"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"shim test build failed:\n{r.stdout}\n{r.stderr}")
+    if verbose and r.stdout.strip():
+        print(r.stdout)
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--oracle", action="store_true", help="also build oracle/")
+    ap.add_argument("--shim-tests", action="store_true", help="also build tests/cpp")
     a = ap.parse_args()
     print(build(force=a.force, verbose=True))
     if a.oracle:
         build_oracle(verbose=True)
+    if a.shim_tests:
+        build_shim_tests(verbose=True)
