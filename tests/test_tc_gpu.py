@@ -209,3 +209,41 @@ def test_rmat18_vs_oracle(cuda):
     want = O.tri_count(optr, oidx)
     with _upload_host(ptr, idx, 1 << 18) as g:
         assert g.count() == want
+
+
+@pytest.mark.parametrize("cfg", [
+    {"warp_tile_cost": 1 << 12, "cta_tile_cost": 1 << 16, "min_blocks": 3},
+    {"warp_tile_cost": 1 << 18, "cta_tile_cost": 1 << 23, "min_blocks": 2},
+    {"warp_tile_cost": 1 << 15, "cta_tile_cost": 1 << 20, "vertex_overhead": 0, "min_blocks": 2},
+])
+def test_tile_shapes_keep_the_count(cuda, cfg):
+    """The scheduler's tile shapes change only how work is cut, never the count."""
+    from gary_b200 import autotune
+
+    src, dst = gb.gen_rmat(16, 21, 32 << 16)
+    ptr, idx = gb.csr_from_edges(src, dst, 1 << 16)
+    optr, oidx = O.orient(ptr, idx)
+    want = O.tri_count(optr, oidx)
+    try:
+        autotune.apply(cfg)
+        with _upload_host(ptr, idx, 1 << 16) as g:
+            assert g.count() == want
+    finally:
+        autotune.apply({})
+
+
+def test_scratch_pool_setting_keeps_results(cuda):
+    """Trimming the library's scratch pool at every sync (pool_keep_bytes 0)
+    and keeping it mapped give the same graph and count."""
+    L = _lib.load()
+    src, dst = gb.gen_rmat(14, 2, 16 << 14)
+    ptr, idx = gb.csr_from_edges(src, dst, 1 << 14)
+    optr, oidx = O.orient(ptr, idx)
+    want = O.tri_count(optr, oidx)
+    try:
+        for keep in (0, (1 << 64) - 1):
+            _lib.check(L.gary_tune(b"pool_keep_bytes", keep), "gary_tune")
+            with _upload_host(ptr, idx, 1 << 14) as g:
+                assert g.count() == want
+    finally:
+        _lib.check(L.gary_tune(b"pool_keep_bytes", (1 << 64) - 1), "gary_tune")
