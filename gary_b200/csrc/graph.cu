@@ -169,7 +169,7 @@ __global__ void k_rows(const uint64_t *__restrict__ rowstart, uint32_t n,
        u += (uint64_t)gridDim.x * blockDim.x) {
     uint32_t d = (uint32_t)(rowstart[u + 1] - rowstart[u]);
     dplus[u] = d;
-    plen4[u] = (d + 3u) >> 2;
+    plen4[u] = ((d + 7u) >> 3) << 1;  // whole octets: 32-byte aligned, padded to 8 words
   }
 }
 

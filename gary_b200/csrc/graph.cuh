@@ -2,10 +2,12 @@
 // (include/DeviceGraph.cuh:75-133).  Owns the degree-oriented adjacency in HBM.
 //
 // A PaddedCSR holds one orientation of the graph:
-//   row[v]    uint2 {off4, len}: list of v starts at adj + 4*off4 (16-byte
-//             aligned), len ids, padded with UINT32_MAX to a multiple of 4 so a
-//             list can be read with uint4 loads and staged with cp.async.bulk
-//             (16-byte granularity) without bounds fixes
+//   row[v]    uint2 {off4, len}: list of v starts at adj + 4*off4 (32-byte
+//             aligned: off4 is even), len ids, padded with UINT32_MAX to a
+//             multiple of 8 so a list can be read as whole 32-byte octets
+//             (one sector, two uint4 loads) that never reach the next list,
+//             and staged with cp.async.bulk (16-byte granularity) without
+//             bounds fixes
 //   indptr[v] uint64 word offset (= 4*off4) and outdeg[v] = len: the
 //             reference's DeviceCSR field layout (DeviceGraph.cuh:15-43)
 //

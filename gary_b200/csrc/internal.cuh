@@ -126,8 +126,8 @@ struct DevBuf {
 };
 
 // ---- kernel-side graph view: one 8-byte row record per vertex -----------
-// row[v] = {off4, len}: v's list starts at adj + 4*off4 (16-byte aligned) and
-// holds len ids, padded with kSentinel up to a multiple of 4.
+// row[v] = {off4, len}: v's list starts at adj + 4*off4 (32-byte aligned) and
+// holds len ids, padded with kSentinel up to a multiple of 8.
 // ranked: ids are degree ranks, so every list is in orientation order and
 // N+(v) holds only ids > v.  Kernels use it to skip list prefixes that cannot
 // close a pattern; with caller ids (GARY_KEEP_IDS) they must not.

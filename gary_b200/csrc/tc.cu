@@ -464,23 +464,17 @@ constexpr uint32_t kWarpBitmapSpan = bitmap_max_span(kWarpTableSlots);  // ids a
 
 // One chunk of at most 32 in-edge records [kb, ke): count the members of each
 // suffix that `set` holds.  Suffixes are read as 32-byte-aligned octets of
-// ids (two 16-byte loads from one sector; the padded layout plus 4 slack
-// words at the end of adj keep every octet in bounds); the lanes walk the
-// concatenation of the chunk's octets, so short suffixes do not idle lanes.
-// Ids of an octet outside the suffix are masked.  All 32 lanes must call.
-// An octet of suffix ids in flight: its 8 words and the valid-word mask.
-struct Octet {
-  uint4 a, b;
-  uint32_t vm;
-};
-
+// ids (two 16-byte loads from one sector); the lanes walk the concatenation of
+// the chunk's octets, so short suffixes do not idle lanes.  Lists start on
+// 32-byte boundaries and are padded with kSentinel to a multiple of 8 words,
+// so an octet only ever holds words of its own list: ids up to and including
+// v before the suffix (all below min N+(v)) and padding.  Every set rejects
+// both as out of its [lo, lo + span] range, so no per-id mask is needed.
+// All 32 lanes must call.
 template <typename Set>
-__device__ __forceinline__ uint32_t probe_octet(const Octet &x, const Set &set) {
-  const uint32_t vm = x.vm;
-  return (set.contains(x.a.x) & vm) + (set.contains(x.a.y) & (vm >> 1)) +
-         (set.contains(x.a.z) & (vm >> 2)) + (set.contains(x.a.w) & (vm >> 3)) +
-         (set.contains(x.b.x) & (vm >> 4)) + (set.contains(x.b.y) & (vm >> 5)) +
-         (set.contains(x.b.z) & (vm >> 6)) + (set.contains(x.b.w) & (vm >> 7));
+__device__ __forceinline__ uint32_t probe_octet(const uint4 &a, const uint4 &b, const Set &set) {
+  return set.contains(a.x) + set.contains(a.y) + set.contains(a.z) + set.contains(a.w) +
+         set.contains(b.x) + set.contains(b.y) + set.contains(b.z) + set.contains(b.w);
 }
 
 template <typename Set>
@@ -488,51 +482,39 @@ __device__ __forceinline__ uint32_t walk_chunk(const uint4 *__restrict__ adj4,
                                                const uint2 *__restrict__ edges, uint64_t kb,
                                                uint64_t ke, int lane, const Set &set) {
   const uint64_t kk = kb + lane;
-  uint32_t s = 0, e = 0, o0 = 0, no = 0;
+  uint32_t o0 = 0, no = 0;
   if (kk < ke) {
     const uint2 r = edges[kk];
-    s = r.x;
-    e = r.x + r.y;
-    o0 = s >> 3;
-    no = ((e + 7) >> 3) - o0;
+    o0 = r.x >> 3;
+    no = ((r.x + r.y + 7) >> 3) - o0;
   }
   const uint32_t incl = warp_inclusive_sum(no, lane);
-  const uint32_t excl = incl - no;
   const uint32_t total = __shfl_sync(kFull, incl, 31);
-  // Locate and load the octet of flattened position pb + lane (all lanes call).
-  auto fetch = [&](uint32_t pb) {
+  if (total == 0) return 0;
+  // flattened position p of record k's octets maps to octet (o0 - excl) + p
+  const uint32_t bias = o0 - (incl - no);
+  auto fetch = [&](uint32_t pb, uint4 &a, uint4 &b) {
     const uint32_t p = pb + lane;
-    const int o = warp_owner(incl, p);
-    const uint32_t ox = __shfl_sync(kFull, excl, o);
-    const uint32_t oo = __shfl_sync(kFull, o0, o);
-    const uint32_t os = __shfl_sync(kFull, s, o);
-    const uint32_t oe = __shfl_sync(kFull, e, o);
-    Octet x;
-    x.vm = 0;
+    const uint32_t oc = __shfl_sync(kFull, bias, warp_owner(incl, p)) + p;
     if (p < total) {
-      const uint32_t oc = oo + (p - ox);
-      x.a = adj4[2 * oc];
-      x.b = adj4[2 * oc + 1];
-      const uint32_t w = oc * 8;
-      // valid ids of this octet: words [max(w, os), min(w + 8, oe))
-      const uint32_t skip = os > w ? os - w : 0u;
-      const uint32_t keep = oe - w < 8u ? oe - w : 8u;
-      x.vm = ((1u << keep) - 1u) & ~((1u << skip) - 1u);
+      a = adj4[2 * oc];
+      b = adj4[2 * oc + 1];
     } else {
-      x.a = x.b = make_uint4(kSentinel, kSentinel, kSentinel, kSentinel);
+      a = b = make_uint4(kSentinel, kSentinel, kSentinel, kSentinel);
     }
-    return x;
   };
   uint32_t cnt = 0;
-  if (total == 0) return 0;
   // two batches in flight: the next octet loads while this one is probed
-  Octet cur = fetch(0);
+  uint4 ca, cb;
+  fetch(0, ca, cb);
   for (uint32_t pb = 32; pb < total; pb += 32) {
-    const Octet nxt = fetch(pb);
-    cnt += probe_octet(cur, set);
-    cur = nxt;
+    uint4 na, nb;
+    fetch(pb, na, nb);
+    cnt += probe_octet(ca, cb, set);
+    ca = na;
+    cb = nb;
   }
-  cnt += probe_octet(cur, set);
+  cnt += probe_octet(ca, cb, set);
   return cnt;
 }
 
@@ -700,7 +682,7 @@ __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 
   } else {
     RegSet8 st;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) st.r[k] = (uint32_t)k < d ? av[k] : kSentinel;
+    for (int k = 0; k < 8; ++k) st.r[k] = av[(uint32_t)k < d ? k : d - 1];  // repeats, never padding
     c = walk_range(adj4, inedge, kb, ke, lane, st);
   }
   __syncwarp();

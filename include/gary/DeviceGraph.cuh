@@ -5,8 +5,8 @@
 // What differs from the reference, and why:
 //   - The views describe the degree-oriented DAG the library builds on upload
 //     (gary_graph_upload): ids are degree ranks unless GARY_KEEP_IDS is given,
-//     lists are sorted, start on 16-byte boundaries and are padded with
-//     GARY_PAD (UINT32_MAX) up to a multiple of 4.  `deg[v]` is the real
+//     lists are sorted, start on 32-byte boundaries and are padded with
+//     GARY_PAD (UINT32_MAX) up to a multiple of 8.  `deg[v]` is the real
 //     length, so N(v) never shows the padding.
 //   - The COO view has its own colIdx (the reference aliases the CSR's,
 //     DeviceGraph.cuh:117, which the padding would break).

@@ -82,9 +82,9 @@ typedef struct gary_graph_info {
 
 /* Raw views with the reference's field names (include/DeviceGraph.cuh:15-67).
  * colIdx + indPtr[v] points at v's oriented list, deg[v] entries long; lists
- * start on 16-byte boundaries and are padded with UINT32_MAX.  The COO view
- * has its own unpadded colIdx (the reference aliases the CSR's,
- * DeviceGraph.cuh:117, which padding would break). */
+ * start on 32-byte boundaries and are padded with UINT32_MAX to a multiple of
+ * 8 ids.  The COO view has its own unpadded colIdx (the reference aliases the
+ * CSR's, DeviceGraph.cuh:117, which padding would break). */
 typedef struct gary_device_csr {
   uint32_t m;
   uint64_t nnz;
@@ -101,7 +101,7 @@ typedef struct gary_device_coo {
   const uint32_t *deg;
 } gary_device_coo;
 
-/* Upload a CSR and build the degree-oriented, 16-byte-aligned, padded uint32
+/* Upload a CSR and build the degree-oriented, 32-byte-aligned, padded uint32
  * lists on the device.  Replaces DeviceGraphCtx::loadFromHost(GraphCSR)
  * (src/DeviceGraph.cu:18-28) plus the host orientation pass
  * (src/Graph.cpp:34-61, convert.cpp:61-78).  Orientation is by (degree, id),

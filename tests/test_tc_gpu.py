@@ -175,7 +175,7 @@ def test_device_views(golden, cuda):
         deg = dev(csr.deg, n, np.uint32)
         assert np.array_equal(deg, np.diff(p.astype(np.int64)).astype(np.uint32))
         indptr = dev(csr.indPtr, n + 1, np.uint64)
-        assert np.all(indptr % 4 == 0)                      # 16-byte aligned lists
+        assert np.all(indptr % 8 == 0)                      # 32-byte aligned lists
         adj = dev(csr.colIdx, int(indptr[-1]), np.uint32)
         for v in range(0, n, 37):
             assert np.array_equal(adj[indptr[v]:indptr[v] + deg[v]], i[p[v]:p[v + 1]])
