@@ -389,13 +389,17 @@ def run_ours(args, dist):
 def run_setops(args, dist):
     """Set-intersection microbench: 2^pairs_log2 pairs of sorted uint32 lists,
     Zipf(1.2) lengths on [1, 65536], values in [0, 2^26), per planted overlap;
-    merge / two-phase search / bitmap, count-only and materialised.  Pairs are
-    generated on the device in batches (not timed); each variant's kernel is
-    timed with CUDA events on every batch."""
+    merge / two-phase search / bitmap / auto, count-only and materialised.
+    Pairs are generated on the device in batches (not timed).  Each variant's
+    kernel is timed with CUDA events on every batch, output buffers prepared
+    beforehand, so the timed region is the one launch.  A batch holds about
+    14 GB of lists, far above L2.  The CPU baseline merges a sample of the first
+    batch's pairs on the host cores (std::set_intersection semantics)."""
     import numpy as np
     import torch
 
     from gary_b200 import setops as so
+    from oracle import oracle as O
 
     torch.cuda.set_device(dist.local)
     cdf = so.zipf_table(65536, 1.2)
@@ -405,30 +409,60 @@ def run_setops(args, dist):
     variants = ["merge", "search", "bitmap", "auto"]
     res = {}
     stream = torch.cuda.Stream()
+    counts = torch.empty(bsz, dtype=torch.int64, device="cuda")
+    tot = torch.zeros(1, dtype=torch.int64, device="cuda")
+    queue = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cpu = None
+    launches = 0
     for ov in overlaps:
         acc = {(v, m): [0.0, 0] for v in variants for m in (False, True)}
         bytes_in = 0
-        out_elems = 0
         for first in range(0, total_pairs, bsz):
             with torch.cuda.stream(stream):
                 batch = so.PairBatch.generate(args.seed, first, bsz, cdf, ov, stream=stream)
+                outs = so.output_buffers(batch)
             stream.synchronize()
             bytes_in += batch.input_bytes()
             for v in variants:
                 for mat in (False, True):
+                    kw = dict(stream=stream, counts=counts, queue=queue, total=tot, outputs=outs if mat else None)
                     with torch.cuda.stream(stream):
-                        so.intersect(batch, so.VARIANTS[v], mat, stream=stream)  # warm
+                        so.intersect(batch, so.VARIANTS[v], mat, **kw)  # warm
                         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                         e0.record(stream)
-                        r = so.intersect(batch, so.VARIANTS[v], mat, stream=stream)
+                        so.intersect(batch, so.VARIANTS[v], mat, **kw)
                         e1.record(stream)
                     stream.synchronize()
+                    launches += 1
                     acc[(v, mat)][0] += e0.elapsed_time(e1)
-                    acc[(v, mat)][1] = acc[(v, mat)][1] + int(r[1].item())
-            del batch
+                    acc[(v, mat)][1] += int(tot.item())
+            if cpu is None and not args.no_cpu:
+                # CPU merge on a sample of this batch, checked against the GPU counts
+                S = min(bsz, 1 << 16)
+                so.intersect(batch, so.VARIANTS["auto"], False, stream=stream, counts=counts, queue=queue, total=tot)
+                stream.synchronize()
+                gpu_counts = counts[:S].cpu().numpy()
+                a_off = batch.a_off[:S + 1].cpu().numpy()
+                b_off = batch.b_off[:S + 1].cpu().numpy()
+                a = batch.a[:int(a_off[-1])].cpu().numpy().view(np.uint32)
+                b = batch.b[:int(b_off[-1])].cpu().numpy().view(np.uint32)
+                la, lb = batch.la[:S].cpu().numpy(), batch.lb[:S].cpu().numpy()
+                threads = os.cpu_count() or 1
+                O.intersect_batch(a_off, la, a, b_off, lb, b, threads)  # warm
+                t0 = time.perf_counter()
+                reps = 0
+                while True:
+                    c_cpu, _ = O.intersect_batch(a_off, la, a, b_off, lb, b, threads)
+                    reps += 1
+                    if time.perf_counter() - t0 > 2.0:
+                        break
+                dt = (time.perf_counter() - t0) / reps
+                assert np.array_equal(c_cpu, gpu_counts), "CPU merge and GPU counts differ"
+                cpu = {"value": S / dt, "unit": "pairs/s", "cores": threads, "kind": "port",
+                       "sample": f"first {S} pairs of the overlap-{ov} batch (merge, OpenMP over pairs), "
+                                 f"counts equal to the GPU's"}
+            del batch, outs
         for (v, mat), (ms, hits) in acc.items():
-            if v == "merge" and not mat:
-                out_elems = hits
             b = bytes_in + (4 * hits if mat else 0)
             res[f"ov{ov}:{v}:{'mat' if mat else 'count'}"] = {
                 "pairs_per_s": total_pairs / (ms / 1e3), "ms": ms, "GB_per_s": b / (ms / 1e3) / 1e9,
@@ -437,12 +471,20 @@ def run_setops(args, dist):
         totals = {k: r["intersection_total"] for k, r in res.items() if k.startswith(f"ov{ov}:")}
         assert len(set(totals.values())) == 1, totals
     best = max((r["pairs_per_s"], k) for k, r in res.items() if k.endswith(":count"))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    bk = res[best[1]]
     line = {"metric": "set-intersection pairs/sec (2^24 Zipf(1.2) pairs)", "value": best[0], "unit": "pairs/s",
-            "best": best[1], "n_gpus": 1, "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "best": best[1], "n_gpus": 1, "steps": len(overlaps), "warmup": 1, "higher_is_better": True,
+            "dtype": "u32", "data": "synthetic",
             "config": {"workload": f"set-intersection microbench, 2^{args.pairs_log2} pairs per overlap, "
                                    f"Zipf(1.2) lengths on [1, 65536], values in [0, 2^26)",
-                       "batch_pairs": bsz, "overlaps": overlaps, "seed": args.seed},
-            "variants": res}
+                       "batch_pairs": bsz, "overlaps": overlaps, "seed": args.seed,
+                       "l2": "inputs larger than L2 (each batch holds ~14 GB of lists)"},
+            "roofline": {"bound": "hbm", "achieved": bk["GB_per_s"], "peak": hbm, "unit": "GB/s",
+                         "frac": bk["GB_per_s"] / hbm, "traffic": None,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
+            "cpu_baseline": cpu, "gpu_launches": launches, "variants": res}
     print(json.dumps(line), flush=True)
     return 0
 

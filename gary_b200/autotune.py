@@ -12,9 +12,10 @@ import json
 
 from ._lib import check, load
 
+# warp_tile_cost 0 = the library's own sizing from the graph's work
 GRID = {
-    "warp_tile_cost": (1 << 13, 1 << 15, 1 << 17),
-    "cta_tile_cost": (1 << 19, 1 << 21),
+    "warp_tile_cost": (0, 1 << 11, 1 << 13, 1 << 15),
+    "cta_tile_cost": (1 << 18, 1 << 20),
     "min_blocks": (2, 3),
 }
 

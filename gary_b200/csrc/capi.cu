@@ -227,10 +227,10 @@ extern "C" int gary_tune(const char *key, uint64_t value) {
   std::lock_guard<std::mutex> lk(gary::g_tuning_mu);
   gary::PlanParams &p = gary::g_tuning;
   const std::string k(key);
-  if (k == "warp_tile_cost" && value > 0) p.warp_tile_cost = value;
+  if (k == "warp_tile_cost") p.warp_tile_cost = value;  // 0: from the work
   else if (k == "cta_tile_cost" && value > 0) p.cta_tile_cost = value;
   else if (k == "vertex_overhead") p.vertex_overhead = value;
-  else if (k == "min_blocks" && (value == 2 || value == 3)) p.min_blocks = (uint32_t)value;
+  else if (k == "min_blocks" && (value == 0 || value == 2 || value == 3)) p.min_blocks = (uint32_t)value;
   else if (k == "pool_keep_bytes") gary::set_pool_keep_bytes(value);
   else if (k == "reset") p = gary::PlanParams{};
   else {

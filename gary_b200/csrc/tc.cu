@@ -365,15 +365,33 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
 
 }  // namespace
 
-int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_count_plan **out,
+PlanParams resolve_params(PlanParams pp, uint64_t total_work) {
+  // Measured on RMAT 18-24: the best warp tile holds about 1/32 of a resident
+  // warp's share of the work (2^11 probes at RMAT-18 up to 2^15 at RMAT-22 and
+  // above; larger tiles leave warps idle at the end, smaller ones pay the
+  // per-tile cost), and a third resident CTA per SM pays for its 40-register
+  // cap from about 2^31 probes (RMAT-22) on.
+  if (pp.min_blocks != 2 && pp.min_blocks != 3) pp.min_blocks = total_work >= (1ull << 31) ? 3 : 2;
+  if (!pp.warp_tile_cost) {
+    const uint64_t slots = (uint64_t)sm_count() * kTcWarps * pp.min_blocks;
+    const uint64_t want = total_work / (slots * 32);
+    uint64_t t = 1ull << 11;
+    while (t < want && t < (1ull << 15)) t <<= 1;
+    pp.warp_tile_cost = t;
+  }
+  return pp;
+}
+
+int build_k3_plan(gary_graph *g, const PlanParams &pp_in, cudaStream_t s, gary_count_plan **out,
                   const float *model) {
   auto plan = std::make_unique<gary_count_plan>();
-  plan->params = pp;
   const uint32_t n = g->n;
   auto pol = thrust::cuda::par_nosync.on(s);
   PhaseTrace tr("triangle plan", s);
   GARY_TRY(build_in_index(g, s, plan->in));
   tr.mark("in-edge index");
+  const PlanParams pp = resolve_params(pp_in, plan->in.total_work);
+  plan->params = pp;
   GARY_TRY(plan->vclass.alloc_persistent(n));
   DevBuf<uint64_t> costV;  // cost of each light vertex, 0 for the others
   DevBuf<uint32_t> kW, kC;
@@ -397,8 +415,8 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp, cudaStream_t s, gary_coun
     k_predict<<<grid_for(n), 128, 0, s>>>(dmodel.p, x.p, legal.p, n, plan->variant.p, pcost.p);
     GARY_CUDA(cudaGetLastError());
     const uint64_t total = thrust::reduce(pol, pcost.p, pcost.p + n, 0ull);
-    // about 48 warp tiles per resident warp
-    const uint64_t slots = (uint64_t)sm_count() * 2 * kTcWarps * 48;
+    // about 32 warp tiles per resident warp, in predicted cycles
+    const uint64_t slots = (uint64_t)sm_count() * pp.min_blocks * kTcWarps * 32;
     tw = std::max<uint64_t>(total / std::max<uint64_t>(slots, 1), 4096);
     plan->learned = true;
   }

@@ -36,13 +36,20 @@ struct Tile {
   uint32_t v0, v1, j0, j1;
 };
 
+// warp_tile_cost and min_blocks left at 0 follow the graph's total work
+// (resolve_params): about 32 warp tiles per resident warp, and 3 resident CTAs
+// per SM once there are 2^31 probes or more.
 struct PlanParams {
   uint32_t warp_cap = kWarpTableSlots / 2;  // largest d+(v) a warp set takes
-  uint64_t warp_tile_cost = 1u << 15;       // target probes per warp tile
+  uint64_t warp_tile_cost = 0;              // target probes per warp tile (0: from the work)
   uint64_t cta_tile_cost = 1u << 20;        // target probes per CTA tile
   uint64_t vertex_overhead = 64;            // fixed cost of a middle vertex
-  uint32_t min_blocks = 2;                  // resident CTAs per SM the kernel is built for
+  uint32_t min_blocks = 0;                  // resident CTAs per SM, 2 or 3 (0: from the work)
 };
+
+// The parameters a plan over `total_work` probes uses: explicit values as
+// given, the zeros resolved.
+PlanParams resolve_params(PlanParams pp, uint64_t total_work);
 
 // Process-wide tuning overrides (0 = keep the default), set by gary_tune().
 PlanParams tuned_params();

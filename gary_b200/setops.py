@@ -93,22 +93,33 @@ class PairBatch:
         return 4 * (int(self.la.sum().item()) + int(self.lb.sum().item()))
 
 
+def output_buffers(batch: PairBatch):
+    """(out, out_off) for a materialising pass: pair i may write min(|A_i|, |B_i|)
+    ids from out_off[i]."""
+    import torch
+
+    cap = torch.minimum(batch.la, batch.lb).to(torch.int64)
+    out_off = torch.zeros(batch.npairs + 1, dtype=torch.int64, device=cap.device)
+    torch.cumsum(cap, 0, out=out_off[1:])
+    out = torch.empty(max(int(out_off[-1].item()), 1), dtype=torch.int32, device=cap.device)
+    return out, out_off
+
+
 def intersect(batch: PairBatch, variant: int = GARY_ISECT_AUTO, materialise: bool = False,
-              stream=None, counts=None, queue=None):
+              stream=None, counts=None, queue=None, total=None, outputs=None):
     """Per-pair counts (int64 tensor) and total; with materialise also the
-    sorted intersections (out, out_off)."""
+    sorted intersections (out, out_off).  Buffers given by the caller
+    (counts, queue, total, outputs = output_buffers(batch)) are reused, so the
+    call then launches the kernel and nothing else."""
     import torch
 
     dev = "cuda"
     counts = torch.empty(batch.npairs, dtype=torch.int64, device=dev) if counts is None else counts
-    total = torch.zeros(1, dtype=torch.int64, device=dev)
+    total = torch.zeros(1, dtype=torch.int64, device=dev) if total is None else total
     queue = torch.zeros(1, dtype=torch.int64, device=dev) if queue is None else queue
     out = out_off = None
     if materialise:
-        cap = torch.minimum(batch.la, batch.lb).to(torch.int64)
-        out_off = torch.zeros(batch.npairs + 1, dtype=torch.int64, device=dev)
-        torch.cumsum(cap, 0, out=out_off[1:])
-        out = torch.empty(max(int(out_off[-1].item()), 1), dtype=torch.int32, device=dev)
+        out, out_off = output_buffers(batch) if outputs is None else outputs
     check(load().gary_intersect_batch(
         batch.npairs, batch.a_off.data_ptr(), batch.la.data_ptr(), batch.a.data_ptr(),
         batch.b_off.data_ptr(), batch.lb.data_ptr(), batch.b.data_ptr(), variant, counts.data_ptr(),

@@ -205,10 +205,13 @@ int gary_gen_ba(uint32_t n, uint32_t m, uint64_t seed, uint32_t *src, uint32_t *
 /* ---- tuning (the autotuner's knobs) -------------------------------------
  * Process-wide parameters of the counting plans, applied to plans built after
  * the call (gary_graph_drop_plans discards a graph's cached plans):
- *   "warp_tile_cost"  target probes per warp tile        (default 2^15)
+ *   "warp_tile_cost"  target probes per warp tile; 0 (the default) sizes
+ *                     it from the graph's work: about 32 tiles per resident
+ *                     warp, between 2^11 and 2^15 probes
  *   "cta_tile_cost"   target probes per CTA tile         (default 2^20)
  *   "vertex_overhead" fixed cost charged per vertex      (default 64)
- *   "min_blocks"      resident CTAs per SM, 2 or 3       (default 2)
+ *   "min_blocks"      resident CTAs per SM, 2 or 3; 0 (the default) picks 3
+ *                     from 2^31 probes on, else 2
  *   "pool_keep_bytes" freed construction scratch the library's per-device
  *                     memory pool keeps mapped across syncs (default
  *                     UINT64_MAX: all of it, like a caching allocator; 0

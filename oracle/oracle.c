@@ -243,6 +243,23 @@ int64_t orc_intersect(const uint32_t *a, int64_t na, const uint32_t *b, int64_t 
   return c;
 }
 
+/* Per-pair |A_i & B_i| of a pair batch by the same merge, OpenMP over pairs
+ * (the reference's CPU check runs std::set_intersection one pair at a time,
+ * test/SetOpTest.cu:94-95).  Returns the total. */
+uint64_t orc_intersect_batch(int64_t npairs, const int64_t *a_off, const int32_t *la,
+                             const uint32_t *a, const int64_t *b_off, const int32_t *lb,
+                             const uint32_t *b, int64_t *counts, int threads) {
+  uint64_t total = 0;
+  if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
+  for (int64_t p = 0; p < npairs; ++p) {
+    const int64_t c = orc_intersect(a + a_off[p], la[p], b + b_off[p], lb[p], NULL);
+    if (counts) counts[p] = c;
+    total += (uint64_t)c;
+  }
+  return total;
+}
+
 /* binary_search(span, key), include/ops/Search.cuh:48-61 */
 int orc_binary_search(const uint32_t *list, int64_t n, uint32_t key) {
   int64_t l = 0, r = n - 1;

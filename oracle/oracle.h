@@ -58,6 +58,11 @@ void orc_tc_bytes(uint32_t n, const uint64_t *ptr, const uint32_t *idx, uint64_t
 int64_t orc_intersect(const uint32_t *a, int64_t na, const uint32_t *b, int64_t nb,
                       uint32_t *out /* may be NULL: count only */);
 
+/* orc_intersect over a batch of pairs, OpenMP over pairs; counts may be NULL. */
+uint64_t orc_intersect_batch(int64_t npairs, const int64_t *a_off, const int32_t *la,
+                             const uint32_t *a, const int64_t *b_off, const int32_t *lb,
+                             const uint32_t *b, int64_t *counts, int threads);
+
 /* binary_search (include/ops/Search.cuh:48-61) */
 int orc_binary_search(const uint32_t *list, int64_t n, uint32_t key);
 /* build_cache (Search.cuh:93-100): cache[i] = list[i*n/N], 64-bit index math */

@@ -32,6 +32,7 @@ _ORC = {
     "orc_c4_hom": (_U64, [_U32, _P, _P]),
     "orc_tc_bytes": (None, [_U32, _P, _P, C.POINTER(_U64), C.POINTER(_U64)]),
     "orc_intersect": (_I64, [_P, _I64, _P, _I64, _P]),
+    "orc_intersect_batch": (_U64, [_I64, _P, _P, _P, _P, _P, _P, _P, _INT]),
     "orc_binary_search": (_INT, [_P, _I64, _U32]),
     "orc_build_cache": (None, [_P, _I64, _INT, _P]),
     "orc_binary_search_2phase": (_INT, [_P, _I64, _P, _INT, _U32]),
@@ -154,6 +155,18 @@ def intersect(a, b, materialise: bool = False):
     out = np.zeros(max(min(len(a), len(b)), 1), np.uint32) if materialise else None
     k = orc().orc_intersect(a.ctypes.data, len(a), b.ctypes.data, len(b), out.ctypes.data if materialise else None)
     return out[:k].copy() if materialise else int(k)
+
+
+def intersect_batch(a_off, la, a, b_off, lb, b, threads: int = 0):
+    """(per-pair counts, total) by merge over a pair batch, OpenMP over pairs."""
+    a_off, b_off = _a(a_off, np.int64), _a(b_off, np.int64)
+    la, lb = _a(la, np.int32), _a(lb, np.int32)
+    a, b = _a(a, np.uint32), _a(b, np.uint32)
+    counts = np.zeros(len(la), np.int64)
+    t = orc().orc_intersect_batch(len(la), a_off.ctypes.data, la.ctypes.data, a.ctypes.data,
+                                  b_off.ctypes.data, lb.ctypes.data, b.ctypes.data, counts.ctypes.data,
+                                  threads)
+    return counts, int(t)
 
 
 def binary_search(lst, keys) -> np.ndarray:
