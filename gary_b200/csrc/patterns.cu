@@ -18,9 +18,16 @@
 //   c(u,w) = |{v < u : v adjacent to u and to w}|.
 // The wedges u-v-w (v, w < u) are walked and c(u,w) is accumulated in a
 // counter map; adding the counter's old value at every increment sums
-// C(c, 2) directly.  Warps use a shared-memory map; vertices with more
-// wedges than it holds use a per-CTA dense counter array in HBM that is
-// reset by a second walk.
+// C(c, 2) directly.  Three classes of u by wedge count:
+//   light  (<= 512)    a warp's shared hash map;
+//   medium (<= 8192)   a CTA's shared hash map;
+//   heavy              dense counters in shared memory over windows of
+//                      48 K consecutive w ids.  Each v keeps a cursor into
+//                      N(v) (sorted), so a window pass reads exactly the ids
+//                      that fall in it; windows nothing reaches are skipped,
+//                      and a heavy u is cut into tiles of consecutive windows
+//                      that different CTAs take.
+// All counter traffic stays in shared memory; the lists stream from HBM.
 #include <thrust/binary_search.h>
 #include <thrust/copy.h>
 #include <thrust/execution_policy.h>
@@ -28,6 +35,8 @@
 #include <thrust/iterator/transform_iterator.h>
 #include <thrust/reduce.h>
 #include <thrust/scan.h>
+#include <thrust/sort.h>
+#include <thrust/transform_reduce.h>
 
 #include <algorithm>
 #include <memory>
@@ -294,49 +303,206 @@ __global__ void __launch_bounds__(kPWarps * 32)
   if (lane == 0 && acc) atomicAdd(out, acc);
 }
 
-// Vertices with more wedges than a warp map holds: the whole CTA walks them
-// against a dense counter array of n words owned by this CTA (pool slot
-// blockIdx.x, all zero between vertices), then walks them again to reset it.
-__global__ void __launch_bounds__(kPWarps * 32)
-    k_c4_big(GraphView s, const uint32_t *__restrict__ dplus, const uint32_t *__restrict__ big,
-             uint32_t n_big, uint32_t *__restrict__ pool, SchedState *sched,
-             unsigned long long *__restrict__ out) {
+// ---- C4, medium vertices: one CTA-wide shared hash map per vertex ---------
+constexpr uint32_t kMidSlots = 16384;  // keys + counts: 128 KiB of shared memory
+constexpr int kMidLog = 14;
+constexpr int kMidThreads = 512;
+constexpr uint64_t kMidWedges = kMidSlots / 2;  // wedges (>= distinct w) a medium vertex may have
+
+__global__ void __launch_bounds__(kMidThreads, 1)
+    k_c4_mid(GraphView s, const uint32_t *__restrict__ dplus, const uint32_t *__restrict__ mid,
+             uint32_t n_mid, SchedState *sched, unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  uint32_t *keys = sm, *vals = sm + kMidSlots;
   __shared__ uint32_t s_u, s_next;
   const int lane = threadIdx.x & 31;
-  uint32_t *cnt = pool + (uint64_t)blockIdx.x * s.n;
   unsigned long long acc = 0;
+  for (uint32_t i = threadIdx.x; i < kMidSlots; i += blockDim.x) {
+    keys[i] = kSentinel;
+    vals[i] = 0;
+  }
   while (true) {
     if (threadIdx.x == 0) {
-      s_u = atomicAdd(&sched->next_cta, 1u);
+      s_u = atomicAdd(&sched->next_aux, 1u);
       s_next = 0;
     }
     __syncthreads();
-    if (s_u >= n_big) break;
-    const uint32_t u = big[s_u];
+    if (s_u >= n_mid) break;
+    const uint32_t u = mid[s_u];
     const uint2 ru = s.row[u];
     const uint32_t pre = ru.y - dplus[u];
     const uint32_t *au = s.adj + (uint64_t)ru.x * 4;
-    // pass 1: count, claiming 32 middle vertices at a time
     while (true) {
       uint32_t k = 0;
       if (lane == 0) k = atomicAdd(&s_next, 32u);
       k = __shfl_sync(kFull, k, 0);
       if (k >= pre) break;
-      c4_wedges(s, au, u, k, min(k + 32, pre), 32, lane,
-                [&](uint32_t w) { acc += atomicAdd(&cnt[w], 1u); });
+      c4_wedges(s, au, u, k, min(k + 32, pre), 32, lane, [&](uint32_t w) {
+        acc += map_incr(keys, vals, kMidSlots - 1, 32 - kMidLog, w);
+      });
     }
     __syncthreads();
-    if (threadIdx.x == 0) s_next = 0;
+    for (uint32_t i = threadIdx.x; i < kMidSlots; i += blockDim.x) {
+      keys[i] = kSentinel;
+      vals[i] = 0;
+    }
+    // the loop head's barrier orders this reset before the next vertex
+  }
+  acc = warp_sum_u64(acc);
+  if (lane == 0 && acc) atomicAdd(out, acc);
+}
+
+// ---- C4, heavy vertices: dense counters over windows of w ids ---------------
+constexpr uint32_t kWinWords = 48 * 1024;  // counters per window: 192 KiB of shared memory
+constexpr int kWinThreads = 1024;
+constexpr int kWinWarps = kWinThreads / 32;
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *l, uint32_t b, uint32_t e,
+                                                    uint32_t x) {
+  while (b < e) {
+    const uint32_t m = (b + e) >> 1;
+    if (l[m] < x) b = m + 1;
+    else e = m;
+  }
+  return b;
+}
+
+// First index i in [c, len) with l[i] >= x (len when none), galloping from c:
+// cheap when the answer is near c, as it is for a cursor moving one window on.
+__device__ __forceinline__ uint32_t gallop_geq(const uint32_t *l, uint32_t c, uint32_t len,
+                                               uint32_t x) {
+  if (c >= len || l[c] >= x) return c;
+  uint32_t b = c, step = 1;  // l[b] < x
+  while ((uint64_t)b + step < len && l[b + step] < x) {
+    b += step;
+    step <<= 1;
+  }
+  const uint64_t e = (uint64_t)b + step < len ? (uint64_t)b + step : len;
+  return lower_bound_u32(l, b + 1, (uint32_t)e, x);
+}
+
+__device__ __forceinline__ uint32_t warp_min_u32(uint32_t x) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) x = min(x, __shfl_xor_sync(kFull, x, o));
+  return x;
+}
+
+// Walk, for the 32 list ranges [b_k, e_k) of the lanes' v's, every id w of
+// N(v_k) in that range (flattened across the lanes); call f(w).  All lanes call.
+template <typename F>
+__device__ __forceinline__ void walk_ranges(const uint32_t *__restrict__ adj, uint32_t q4, uint32_t b,
+                                            uint32_t e, int lane, F f) {
+  const uint32_t len = e - b;
+  const uint32_t incl = warp_inclusive_sum(len, lane);
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  const uint32_t shift = b - (incl - len);  // word of flattened position p: q4*4 + shift + p
+  for (uint32_t pb = 0; pb < total; pb += 32) {
+    const uint32_t p = pb + lane;
+    const int o = warp_owner(incl, p);
+    const uint32_t oq = __shfl_sync(kFull, q4, o);
+    const uint32_t os = __shfl_sync(kFull, shift, o);
+    if (p < total) f(adj[(uint64_t)oq * 4 + (uint32_t)(os + p)]);
+  }
+}
+
+// Tile {v0 = u, v1 = pre, j0 = wa, j1 = wb}: windows [wa, wb) of vertex u,
+// i.e. wedge ends w in [wa * kWinWords, min(wb * kWinWords, u)).
+__global__ void __launch_bounds__(kWinThreads, 1)
+    k_c4_win(GraphView s, const Tile *__restrict__ tiles, uint32_t t_lo, uint32_t t_hi,
+             uint32_t *__restrict__ cursors, uint32_t max_pre, SchedState *sched,
+             unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) uint32_t cnt[];  // kWinWords counters, zero between windows
+  __shared__ uint32_t s_tile, s_next, s_nextw;
+  __shared__ unsigned long long s_wedges;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *cur = cursors + (uint64_t)blockIdx.x * 2 * max_pre, *prev = cur + max_pre;
+  unsigned long long acc = 0;
+  for (uint32_t i = threadIdx.x; i < kWinWords; i += blockDim.x) cnt[i] = 0;
+  while (true) {
+    if (threadIdx.x == 0) {
+      s_tile = t_lo + atomicAdd(&sched->next_cta, 1u);
+      s_nextw = kSentinel;
+    }
     __syncthreads();
-    // pass 2: reset the counters this vertex touched
+    const uint32_t t = s_tile;
+    if (t >= t_hi) break;
+    const Tile tl = tiles[t];
+    const uint32_t u = tl.v0, pre = tl.v1;
+    const uint32_t *au = s.adj + (uint64_t)s.row[u].x * 4;
+    const uint64_t end64 = (uint64_t)tl.j1 * kWinWords, begin64 = (uint64_t)tl.j0 * kWinWords;
+    const uint32_t w_end = end64 < u ? (uint32_t)end64 : u;
+    const uint32_t w_begin = begin64 < w_end ? (uint32_t)begin64 : w_end;
+    // cursors at the tile's first window; the smallest id any of them sees
+    uint32_t first = kSentinel;
+    for (uint32_t i = threadIdx.x; i < pre; i += blockDim.x) {
+      const uint2 rv = s.row[au[i]];
+      const uint32_t *l = s.adj + (uint64_t)rv.x * 4;
+      const uint32_t c = lower_bound_u32(l, 0, rv.y, w_begin);
+      cur[i] = c;
+      if (c < rv.y) first = min(first, l[c]);
+    }
+    first = warp_min_u32(first);
+    if (lane == 0) atomicMin(&s_nextw, first);
+    __syncthreads();
     while (true) {
-      uint32_t k = 0;
-      if (lane == 0) k = atomicAdd(&s_next, 32u);
-      k = __shfl_sync(kFull, k, 0);
-      if (k >= pre) break;
-      c4_wedges(s, au, u, k, min(k + 32, pre), 32, lane, [&](uint32_t w) { cnt[w] = 0u; });
+      const uint32_t nw = s_nextw;
+      if (nw >= w_end) break;  // no id of the tile's range is left
+      const uint32_t lo = nw - nw % kWinWords;
+      const uint32_t hi = lo + kWinWords < w_end ? lo + kWinWords : w_end;
+      __syncthreads();  // every thread has read s_nextw
+      if (threadIdx.x == 0) {
+        s_next = 0;
+        s_nextw = kSentinel;
+        s_wedges = 0;
+      }
+      __syncthreads();
+      // count: advance every cursor past the window, counting the ids passed
+      uint32_t nxt = kSentinel;
+      unsigned long long seen = 0;
+      while (true) {
+        uint32_t k0 = 0;
+        if (lane == 0) k0 = atomicAdd(&s_next, 32u);
+        k0 = __shfl_sync(kFull, k0, 0);
+        if (k0 >= pre) break;
+        const uint32_t k = k0 + lane;
+        uint32_t q4 = 0, b = 0, e = 0;
+        if (k < pre) {
+          const uint2 rv = s.row[au[k]];
+          const uint32_t *l = s.adj + (uint64_t)rv.x * 4;
+          b = cur[k];
+          e = gallop_geq(l, b, rv.y, hi);
+          prev[k] = b;
+          cur[k] = e;
+          q4 = rv.x;
+          if (e < rv.y) nxt = min(nxt, l[e]);
+          seen += e - b;
+        }
+        walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { acc += atomicAdd(&cnt[w - lo], 1u); });
+      }
+      nxt = warp_min_u32(nxt);
+      seen = warp_sum_u64(seen);
+      if (lane == 0) {
+        atomicMin(&s_nextw, nxt);
+        if (seen) atomicAdd(&s_wedges, seen);
+      }
+      __syncthreads();
+      // zero the window again: walk the same ids when few, else clear it whole
+      if (s_wedges + pre < (hi - lo) / 4) {
+        for (uint32_t k0 = warp * 32; k0 < pre; k0 += kWinWarps * 32) {
+          const uint32_t k = k0 + lane;
+          uint32_t q4 = 0, b = 0, e = 0;
+          if (k < pre) {
+            q4 = s.row[au[k]].x;
+            b = prev[k];
+            e = cur[k];
+          }
+          walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { cnt[w - lo] = 0u; });
+        }
+      } else {
+        for (uint32_t i = threadIdx.x; i < hi - lo; i += blockDim.x) cnt[i] = 0;
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   acc = warp_sum_u64(acc);
   if (lane == 0 && acc) atomicAdd(out, acc);
@@ -434,6 +600,92 @@ __global__ void k_c4_classify(const uint2 *__restrict__ srow, const uint32_t *__
   }
 }
 
+// Exact wedge count of each listed vertex: sum over v in N(u), v < u, of
+// |N(v) below u|.  One warp per vertex.
+__global__ void k_c4_exact_wedges(const uint2 *__restrict__ srow, const uint32_t *__restrict__ sadj,
+                                  const uint32_t *__restrict__ dplus, const uint32_t *__restrict__ list,
+                                  uint32_t nl, uint64_t *__restrict__ wed) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nl; i += warps) {
+    const uint32_t u = list[i];
+    const uint2 ru = srow[u];
+    const uint32_t pre = ru.y - dplus[u];
+    uint64_t w = 0;
+    for (uint32_t k = lane; k < pre; k += 32) {
+      const uint2 rv = srow[sadj[(uint64_t)ru.x * 4 + k]];
+      w += prefix_below(sadj + (uint64_t)rv.x * 4, rv.y, u);
+    }
+    w = warp_sum_u64(w);
+    if (lane == 0) wed[i] = w;
+  }
+}
+
+__host__ __device__ __forceinline__ uint32_t c4_windows(uint32_t u) {
+  return (uint32_t)(((uint64_t)u + kWinWords - 1) / kWinWords);
+}
+
+// Cost of a heavy vertex in probe units: its wedges, a cursor step per
+// (window, v), a barrier-bound overhead per window.
+__global__ void k_c4_heavy_cost(const uint2 *__restrict__ srow, const uint32_t *__restrict__ dplus,
+                                const uint32_t *__restrict__ heavy, const uint64_t *__restrict__ wed,
+                                uint32_t nh, uint64_t *__restrict__ cost) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nh;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = heavy[i];
+    const uint32_t pre = srow[u].y - dplus[u];
+    const uint64_t nw = c4_windows(u);
+    cost[i] = wed[i] + nw * (2ull * pre + 4096);
+  }
+}
+
+__global__ void k_c4_tile_counts(const uint32_t *__restrict__ heavy, const uint64_t *__restrict__ cost,
+                                 uint32_t nh, uint64_t target, uint32_t *__restrict__ kt) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nh;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t want = (cost[i] + target - 1) / target;
+    const uint64_t nw = c4_windows(heavy[i]);
+    kt[i] = (uint32_t)(want < 1 ? 1 : (want > nw ? nw : want));
+  }
+}
+
+__global__ void k_c4_fill_tiles(const uint2 *__restrict__ srow, const uint32_t *__restrict__ dplus,
+                                const uint32_t *__restrict__ heavy, uint32_t nh,
+                                const uint32_t *__restrict__ off, Tile *__restrict__ tiles) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nh;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = heavy[i];
+    const uint32_t pre = srow[u].y - dplus[u];
+    const uint32_t kk = off[i + 1] - off[i];
+    const uint64_t nw = c4_windows(u);
+    for (uint32_t j = 0; j < kk; ++j) {
+      Tile t;
+      t.v0 = u;
+      t.v1 = pre;
+      t.j0 = (uint32_t)(nw * j / kk);
+      t.j1 = (uint32_t)(nw * (j + 1) / kk);
+      tiles[off[i] + j] = t;
+    }
+  }
+}
+
+struct AtMost {
+  uint64_t cap;
+  __host__ __device__ bool operator()(uint64_t w) const { return w <= cap; }
+};
+struct Above {
+  uint64_t cap;
+  __host__ __device__ bool operator()(uint64_t w) const { return w > cap; }
+};
+struct PreOf {
+  const uint2 *srow;
+  const uint32_t *dplus;
+  __host__ __device__ uint32_t operator()(uint32_t u) const { return srow[u].y - dplus[u]; }
+};
+struct MaxU32 {
+  __host__ __device__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
+};
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -528,17 +780,59 @@ int build_c4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
                                                  kPSlots / 2, cls.p);
   GARY_CUDA(cudaGetLastError());
   GARY_TRY(plan->light.alloc_persistent(std::max<uint32_t>(n, 1)));
-  GARY_TRY(plan->big.alloc_persistent(std::max<uint32_t>(n, 1)));
   plan->n_light = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
                                              thrust::counting_iterator<uint32_t>(n), plan->light.p,
                                              ClassIs{cls.p, kClassLight}) - plan->light.p);
-  plan->n_big = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
-                                           thrust::counting_iterator<uint32_t>(n), plan->big.p,
-                                           ClassIs{cls.p, kClassCta}) - plan->big.p);
-  plan->pool_ctas = std::min<uint32_t>(plan->n_big, (uint32_t)sm_count());
-  if (plan->pool_ctas) {
-    GARY_TRY(plan->pool.alloc_persistent((uint64_t)plan->pool_ctas * n));
-    GARY_CUDA(cudaMemsetAsync(plan->pool.p, 0, plan->pool.bytes(), s));
+  // the rest: exact wedge counts, then medium (a CTA hash map) or heavy (windows)
+  DevBuf<uint32_t> big;
+  GARY_TRY(big.alloc(std::max<uint32_t>(n, 1), s));
+  const uint32_t nb = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                                 thrust::counting_iterator<uint32_t>(n), big.p,
+                                                 ClassIs{cls.p, kClassCta}) - big.p);
+  DevBuf<uint64_t> wed;
+  GARY_TRY(wed.alloc(std::max<uint32_t>(nb, 1), s));
+  if (nb) {
+    k_c4_exact_wedges<<<grid_for((uint64_t)nb * 32), kThreads, 0, s>>>(g->sym.row.p, g->sym.adj.p,
+                                                                       g->dag.outdeg.p, big.p, nb, wed.p);
+    GARY_CUDA(cudaGetLastError());
+  }
+  GARY_TRY(plan->mid.alloc_persistent(std::max<uint32_t>(nb, 1)));
+  plan->n_mid = (uint32_t)(thrust::copy_if(pol, big.p, big.p + nb, wed.p, plan->mid.p,
+                                           AtMost{kMidWedges}) - plan->mid.p);
+  DevBuf<uint32_t> heavy;
+  DevBuf<uint64_t> cost;
+  GARY_TRY(heavy.alloc(std::max<uint32_t>(nb, 1), s));
+  const uint32_t nh = (uint32_t)(thrust::copy_if(pol, big.p, big.p + nb, wed.p, heavy.p,
+                                                 Above{kMidWedges}) - heavy.p);
+  GARY_TRY(cost.alloc(std::max<uint32_t>(nh, 1), s));
+  plan->win_ctas = (uint32_t)sm_count();
+  if (nh) {
+    DevBuf<uint64_t> hw;
+    GARY_TRY(hw.alloc(nh, s));
+    thrust::copy_if(pol, wed.p, wed.p + nb, wed.p, hw.p, Above{kMidWedges});
+    k_c4_heavy_cost<<<grid_for(nh), kThreads, 0, s>>>(g->sym.row.p, g->dag.outdeg.p, heavy.p, hw.p,
+                                                      nh, cost.p);
+    GARY_CUDA(cudaGetLastError());
+    // biggest vertices first; tiles of about 1/8 of a CTA's share of the work
+    thrust::sort_by_key(pol, cost.p, cost.p + nh, heavy.p, thrust::greater<uint64_t>());
+    const uint64_t total = thrust::reduce(pol, cost.p, cost.p + nh, 0ull);
+    const uint64_t target = std::max<uint64_t>(total / ((uint64_t)plan->win_ctas * 8), 1ull << 22);
+    DevBuf<uint32_t> kt;
+    GARY_TRY(kt.alloc((uint64_t)nh + 1, s));
+    k_c4_tile_counts<<<grid_for(nh), kThreads, 0, s>>>(heavy.p, cost.p, nh, target, kt.p);
+    GARY_CUDA(cudaMemsetAsync(kt.p + nh, 0, 4, s));
+    thrust::exclusive_scan(pol, kt.p, kt.p + nh + 1, kt.p, 0u);
+    uint32_t nt = 0;
+    GARY_CUDA(cudaMemcpyAsync(&nt, kt.p + nh, 4, cudaMemcpyDeviceToHost, s));
+    plan->max_pre = thrust::transform_reduce(pol, heavy.p, heavy.p + nh,
+                                             PreOf{g->sym.row.p, g->dag.outdeg.p}, 0u, MaxU32());
+    GARY_CUDA(cudaStreamSynchronize(s));
+    plan->n_cta = nt;
+    GARY_TRY(plan->tiles.alloc_persistent(std::max<uint32_t>(nt, 1)));
+    k_c4_fill_tiles<<<grid_for(nh), kThreads, 0, s>>>(g->sym.row.p, g->dag.outdeg.p, heavy.p, nh, kt.p,
+                                                      plan->tiles.p);
+    GARY_CUDA(cudaGetLastError());
+    GARY_TRY(plan->cursors.alloc_persistent((uint64_t)plan->win_ctas * 2 * std::max(plan->max_pre, 1u)));
   }
   GARY_TRY(plan->sched.alloc_persistent(1));
   GARY_CUDA(cudaStreamSynchronize(s));
@@ -548,36 +842,43 @@ int build_c4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
 
 int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaStream_t s,
               uint32_t shard, uint32_t nshards) {
-  // shards split the light list and the big list
-  const uint32_t l0 = (uint32_t)((uint64_t)plan->n_light * shard / nshards);
-  const uint32_t l1 = (uint32_t)((uint64_t)plan->n_light * (shard + 1) / nshards);
-  const uint32_t b0 = (uint32_t)((uint64_t)plan->n_big * shard / nshards);
-  const uint32_t b1 = (uint32_t)((uint64_t)plan->n_big * (shard + 1) / nshards);
-  const size_t smem = (size_t)kPWarps * 2 * kPSlots * 4;
+  // shards split the heavy tiles, the medium list and the light list
+  auto part = [&](uint32_t total, uint32_t k) { return (uint32_t)((uint64_t)total * k / nshards); };
+  const uint32_t t0 = part(plan->n_cta, shard), t1 = part(plan->n_cta, shard + 1);
+  const uint32_t m0 = part(plan->n_mid, shard), m1 = part(plan->n_mid, shard + 1);
+  const uint32_t l0 = part(plan->n_light, shard), l1 = part(plan->n_light, shard + 1);
+  const size_t smem_small = (size_t)kPWarps * 2 * kPSlots * 4;
+  const size_t smem_mid = (size_t)2 * kMidSlots * 4;
+  const size_t smem_win = (size_t)kWinWords * 4;
   static bool attr[64] = {false};
   const int dev = device_ordinal();
   if (dev < 64 && !attr[dev]) {
-    GARY_CUDA(cudaFuncSetAttribute(k_c4_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GARY_CUDA(cudaFuncSetAttribute(k_c4_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_small));
+    GARY_CUDA(cudaFuncSetAttribute(k_c4_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mid));
+    GARY_CUDA(cudaFuncSetAttribute(k_c4_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_win));
     attr[dev] = true;
   }
   int per_sm = 0;
-  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_small, kPWarps * 32, smem));
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_small, kPWarps * 32, smem_small));
   if (per_sm < 1) per_sm = 1;
   const GraphView sv{g->n, g->sym.row.p, g->sym.adj.p, true};
   GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
   GARY_CUDA(cudaMemsetAsync(d_out, 0, 8, s));
   GARY_CUDA(cudaEventRecord(g->ev0, s));
-  if (b1 > b0)
-    k_c4_big<<<std::min<uint32_t>(plan->pool_ctas, b1 - b0), kPWarps * 32, 0, s>>>(
-        sv, g->dag.outdeg.p, plan->big.p + b0, b1 - b0, plan->pool.p, plan->sched.p, d_out);
+  if (t1 > t0)
+    k_c4_win<<<std::min<uint32_t>(plan->win_ctas, t1 - t0), kWinThreads, smem_win, s>>>(
+        sv, plan->tiles.p, t0, t1, plan->cursors.p, std::max(plan->max_pre, 1u), plan->sched.p, d_out);
+  if (m1 > m0)
+    k_c4_mid<<<std::min<uint32_t>((uint32_t)sm_count(), m1 - m0), kMidThreads, smem_mid, s>>>(
+        sv, g->dag.outdeg.p, plan->mid.p + m0, m1 - m0, plan->sched.p, d_out);
   if (l1 > l0)
-    k_c4_small<<<(unsigned)(sm_count() * per_sm), kPWarps * 32, smem, s>>>(
+    k_c4_small<<<(unsigned)(sm_count() * per_sm), kPWarps * 32, smem_small, s>>>(
         sv, g->dag.outdeg.p, plan->light.p + l0, l1 - l0, plan->sched.p, d_out);
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
-  g->last.tiles = (l1 - l0) + (b1 - b0);
-  g->last.cta_tiles = b1 - b0;
+  g->last.tiles = (t1 - t0) + (m1 - m0) + (l1 - l0);
+  g->last.cta_tiles = (t1 - t0) + (m1 - m0);
   g->last_timed = true;
   return GARY_OK;
 }

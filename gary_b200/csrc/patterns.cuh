@@ -11,12 +11,14 @@ namespace gary {
 constexpr uint32_t kK4MaxOutDegree = 4096;
 
 struct PatternPlan {
-  DevBuf<Tile> tiles;      // K4: CTA tiles then warp tiles
-  DevBuf<uint32_t> light;  // light vertices (K4 groups index it; C4 warps walk it)
-  DevBuf<uint32_t> big;    // C4: vertices walked by a whole CTA
-  DevBuf<uint32_t> pool;   // C4: pool_ctas dense counter arrays of n words
+  // K4: CTA tiles then warp tiles.  C4: window tiles of heavy vertices, as
+  // {v0 = u, v1 = |N(u) below u|, j0 = first window, j1 = end window}.
+  DevBuf<Tile> tiles;
+  DevBuf<uint32_t> light;    // light vertices (K4 groups index it; C4 warps walk it)
+  DevBuf<uint32_t> mid;      // C4: medium vertices, one CTA hash map each
+  DevBuf<uint32_t> cursors;  // C4: per window-kernel CTA, 2 x max_pre list positions
   DevBuf<SchedState> sched;
-  uint32_t n_cta = 0, n_warp = 0, n_light = 0, n_big = 0, pool_ctas = 0;
+  uint32_t n_cta = 0, n_warp = 0, n_light = 0, n_mid = 0, max_pre = 0, win_ctas = 0;
 };
 
 int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out);

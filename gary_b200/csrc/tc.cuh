@@ -74,7 +74,7 @@ struct SchedState {
   uint32_t next_cta;
   uint32_t next_warp;
   uint32_t error;
-  uint32_t pad;
+  uint32_t next_aux;  // a third queue (the 4-cycle kernel's medium vertices)
 };
 
 // In-edge index of the middle-vertex formulation.  For every oriented edge
