@@ -3,14 +3,17 @@
 // defines it; these kernels are new, pinned by the CPU oracle and closed-form
 // known answers.
 //
-// 4-cliques (degree-ranked DAG, every list in orientation order):
-//   K4 = sum over u, over v in N+(u), over w in S = N+(u) & N+(v) of |S & N+(w)|
-// counts each clique u < v < w < x once.  One warp (or CTA) holds N+(u) as a
-// shared hash set whose slots carry one membership bit per warp.  For each
-// middle vertex v it streams N+(v) three times: (A) mark the members of S,
-// (B) for the marked w, walk N+(w) (flattened across the w's of a 32-wide
-// step) counting marked hits, (C) clear the marks.  No buffer for S is
-// needed, so S can be as long as N+(u).
+// 4-cliques (degree-ranked DAG, every list in orientation order): each clique
+// u < v < w < x is counted once at its lowest vertex u, as a triangle of the
+// subgraph induced by N+(u).  For every u (d = d+(u) ids) the kernel builds
+// that subgraph's upper-triangular adjacency as d bit rows of ceil(d/32)
+// words: row i has bit j set when N+(u)[j] is in N+(N+(u)[i]).  Rows are
+// filled by streaming each N+(v), v in N+(u), up to the largest id of N+(u)
+// and looking every id up in a shared id -> position hash of N+(u).  Then
+//   K4(u) = sum over set bits (i, j) of popcount(row_i AND row_j),
+// since row j holds only positions after j.  Vertices with d <= 128 run on
+// one warp (rows of at most 4 words); larger ones take a whole CTA, with
+// rows in shared memory up to d = 1024 and in a per-CTA HBM buffer beyond.
 //
 // 4-cycles (symmetric ranked lists): each cycle is counted once at its
 // highest-ranked vertex u, with w the opposite vertex:
@@ -36,6 +39,7 @@
 #include <thrust/reduce.h>
 #include <thrust/scan.h>
 #include <thrust/sort.h>
+#include <thrust/transform.h>
 #include <thrust/transform_reduce.h>
 
 #include <algorithm>
@@ -51,7 +55,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kPWarps = 8;
 constexpr uint32_t kPSlots = 1024;  // per-warp hash slots
-constexpr uint32_t kCtaSlots = 8192;
 
 inline unsigned grid_for(uint64_t items) {
   uint64_t b = (items + kThreads - 1) / kThreads;
@@ -60,158 +63,6 @@ inline unsigned grid_for(uint64_t items) {
 }
 
 __host__ __device__ __forceinline__ uint64_t min64(uint64_t a, uint64_t b) { return a < b ? a : b; }
-
-// ---- tagged hash set of N+(u) --------------------------------------------
-struct TagSet {
-  uint32_t *keys, *tags;
-  uint32_t mask;
-  int shift;
-  __device__ __forceinline__ int find(uint32_t x) const {
-    uint32_t h = (x * kHashMul) >> shift;
-    while (true) {
-      const uint32_t k = keys[h];
-      if (k == x) return (int)h;
-      if (k == kSentinel) return -1;
-      h = (h + 1) & mask;
-    }
-  }
-};
-
-template <typename Sync>
-__device__ __forceinline__ TagSet build_tagset(const uint32_t *__restrict__ keys_in, uint32_t lo,
-                                               uint32_t hi, uint32_t *keys, uint32_t *tags,
-                                               uint32_t slots, uint32_t tid, uint32_t nthreads,
-                                               Sync sync) {
-  const uint32_t d = hi - lo;
-  int l = d > 1 ? 32 - __clz(2 * d - 1) : 1;
-  const int cap = 31 - __clz(slots);
-  l = l < 5 ? 5 : (l > cap ? cap : l);
-  for (uint32_t i = tid; i < (1u << l); i += nthreads) {
-    keys[i] = kSentinel;
-    tags[i] = 0;
-  }
-  sync();
-  hash_insert_range(keys, l, keys_in, lo, hi, tid, nthreads);
-  sync();
-  return TagSet{keys, tags, (1u << l) - 1, 32 - l};
-}
-
-// K4 work for one (u, v): |S & N+(w)| summed over w in S, S = set & N+(v).
-__device__ uint32_t k4_middle(const GraphView &g, const TagSet &ts, uint32_t v, uint32_t bit,
-                              int lane) {
-  const uint2 rv = g.row[v];
-  const uint32_t dv = rv.y;
-  if (dv < 2) return 0;
-  const uint32_t *av = g.adj + (uint64_t)rv.x * 4;
-  // (A) mark S
-  for (uint32_t k = lane; k < dv; k += 32) {
-    const int sl = ts.find(av[k]);
-    if (sl >= 0) atomicOr(&ts.tags[sl], bit);
-  }
-  __syncwarp();
-  // (B) for every w in S, count marked members of N+(w)
-  uint32_t cnt = 0;
-  for (uint32_t k0 = 0; k0 < dv; k0 += 32) {
-    const uint32_t k = k0 + lane;
-    uint32_t len = 0, base = 0;
-    if (k < dv) {
-      const uint32_t w = av[k];
-      if (ts.find(w) >= 0) {
-        const uint2 rw = g.row[w];
-        len = rw.y;
-        base = rw.x;
-      }
-    }
-    const uint32_t incl = warp_inclusive_sum(len, lane);
-    const uint32_t excl = incl - len;
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    for (uint32_t pb = 0; pb < total; pb += 32) {
-      const uint32_t p = pb + lane;
-      const int o = warp_owner(incl, p);
-      const uint32_t ox = __shfl_sync(kFull, excl, o);
-      const uint32_t ob = __shfl_sync(kFull, base, o);
-      if (p < total) {
-        const int sl = ts.find(g.adj[(uint64_t)ob * 4 + (p - ox)]);
-        cnt += (sl >= 0 && (ts.tags[sl] & bit)) ? 1u : 0u;
-      }
-    }
-  }
-  __syncwarp();
-  // (C) clear the marks
-  for (uint32_t k = lane; k < dv; k += 32) {
-    const int sl = ts.find(av[k]);
-    if (sl >= 0) atomicAnd(&ts.tags[sl], ~bit);
-  }
-  __syncwarp();
-  return cnt;
-}
-
-__global__ void __launch_bounds__(kPWarps * 32)
-    k_k4(GraphView g, const Tile *__restrict__ tiles, const uint32_t *__restrict__ light,
-         uint32_t n_cta, TileRange rng, SchedState *sched, unsigned long long *__restrict__ out) {
-  extern __shared__ __align__(16) uint32_t sm[];
-  __shared__ uint32_t s_tile, s_next;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned long long cnt = 0;
-  // phase 1: CTA tiles (d+(u) beyond a warp table); one shared table, a
-  // membership bit per warp, middle vertices claimed dynamically
-  while (true) {
-    if (threadIdx.x == 0) {
-      s_tile = rng.cta_lo + atomicAdd(&sched->next_cta, 1u);
-      s_next = 0;
-    }
-    __syncthreads();
-    const uint32_t t = s_tile;
-    if (t >= rng.cta_hi) break;
-    const Tile tl = tiles[t];
-    const uint32_t u = tl.v0;
-    const uint2 ru = g.row[u];
-    const uint32_t *au = g.adj + (uint64_t)ru.x * 4;
-    const TagSet ts = build_tagset(au, tl.j0 + 1, ru.y, sm, sm + kCtaSlots, kCtaSlots, threadIdx.x,
-                                   blockDim.x, [] { __syncthreads(); });
-    const uint32_t j1 = min(tl.j1, ru.y - 2);
-    while (true) {
-      uint32_t j = 0;
-      if (lane == 0) j = tl.j0 + atomicAdd(&s_next, 1u);
-      j = __shfl_sync(kFull, j, 0);
-      if (j >= j1) break;
-      cnt += k4_middle(g, ts, au[j], 1u << warp, lane);
-    }
-    __syncthreads();
-  }
-  // phase 2: warp tiles
-  uint32_t *keys = sm + warp * 2 * kPSlots, *tags = keys + kPSlots;
-  const Tile *wt = tiles + n_cta;
-  auto do_u = [&](uint32_t u, uint32_t j0, uint32_t j1) {
-    const uint2 ru = g.row[u];
-    if (ru.y < 3) return;
-    j1 = min(j1, ru.y - 2);
-    if (j0 >= j1) return;
-    const uint32_t *au = g.adj + (uint64_t)ru.x * 4;
-    const TagSet ts = build_tagset(au, j0 + 1, ru.y, keys, tags, kPSlots, lane, 32,
-                                   [] { __syncwarp(); });
-    for (uint32_t j = j0; j < j1; ++j) cnt += k4_middle(g, ts, au[j], 1u, lane);
-    __syncwarp();
-  };
-  while (true) {
-    uint32_t t = 0;
-    if (lane == 0) t = rng.warp_lo + atomicAdd(&sched->next_warp, 1u);
-    t = __shfl_sync(kFull, t, 0);
-    if (t >= rng.warp_hi) break;
-    const Tile tl = wt[t];
-    if (tl.j1 != kGroupTile) {
-      do_u(tl.v0, tl.j0, tl.j1);
-      continue;
-    }
-    for (uint32_t ib = tl.v0; ib < tl.v1; ib += 32) {
-      const uint32_t nb = min(32u, tl.v1 - ib);
-      const uint32_t myu = lane < nb ? light[ib + lane] : 0u;
-      for (uint32_t k = 0; k < nb; ++k) do_u(__shfl_sync(kFull, myu, k), 0, 0xFFFFFFFFu);
-    }
-  }
-  cnt = warp_sum_u64(cnt);
-  if (lane == 0 && cnt) atomicAdd(out, cnt);
-}
 
 // ---- C4 -------------------------------------------------------------------
 // Lower-ranked prefix of v's symmetric list below `u`: lower_bound(N(v), u).
@@ -508,84 +359,156 @@ __global__ void __launch_bounds__(kWinThreads, 1)
   if (lane == 0 && acc) atomicAdd(out, acc);
 }
 
-// ---- plans ------------------------------------------------------------------
-// K4 per-vertex classes: d+(u) >= 3 needed; CTA when d+(u) > warp capacity.
-__global__ void k_k4_classify(const uint2 *__restrict__ row, const uint64_t *__restrict__ wedge,
-                              uint32_t n, uint64_t tw, uint64_t twc, uint8_t *__restrict__ cls,
-                              uint64_t *__restrict__ costL, uint32_t *__restrict__ kW,
-                              uint32_t *__restrict__ kC) {
-  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
-       u += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t d = row[u].y;
-    uint8_t c = kClassNone;
-    uint64_t cl = 0;
-    uint32_t kw = 0, kc = 0;
-    if (d >= 3) {
-      const uint64_t cost = 3 * wedge[u] + 4 * d + 64;
-      const uint32_t span = d - 2;  // middle positions that can close a clique
-      if (d > kPSlots / 2) {
-        c = kClassCta;
-        kc = (uint32_t)min64((cost + twc - 1) / twc, span);
-      } else if (cost > tw) {
-        c = kClassSplit;
-        kw = (uint32_t)min64((cost + tw - 1) / tw, span);
-      } else {
-        c = kClassLight;
-        cl = cost;
+// ---- K4: bit rows of the subgraph induced by N+(u) -------------------------
+constexpr int kK4Threads = 1024;
+constexpr int kK4Warps = kK4Threads / 32;
+constexpr uint32_t kK4SmemWords = 49152;      // 192 KiB
+constexpr uint32_t kK4CtaLog = 13;            // CTA position hash: 8192 slots (d <= 4096)
+constexpr uint32_t kK4CtaRowWords = 32768;    // rows in shared memory when d * W fits
+constexpr uint32_t kK4WarpMaxD = 128;         // warp vertices: rows of at most 4 words
+constexpr uint32_t kK4WarpLog = 8;            // warp position hash: 256 slots
+constexpr uint32_t kK4WarpWords = kK4SmemWords / kK4Warps;  // 1536 words per warp
+static_assert(2 * (1u << kK4WarpLog) + kK4WarpMaxD * (kK4WarpMaxD / 32) <= kK4WarpWords,
+              "warp region too small");
+static_assert(2 * (1u << kK4CtaLog) + kK4CtaRowWords <= kK4SmemWords, "CTA region too small");
+
+__device__ __forceinline__ void pos_insert(uint32_t *keys, uint32_t *pos, uint32_t mask, int shift,
+                                           uint32_t x, uint32_t p) {
+  uint32_t h = (x * kHashMul) >> shift;
+  while (atomicCAS(&keys[h], kSentinel, x) != kSentinel) h = (h + 1) & mask;  // ids are distinct
+  pos[h] = p;
+}
+
+__device__ __forceinline__ int pos_find(const uint32_t *keys, const uint32_t *pos, uint32_t mask,
+                                        int shift, uint32_t x) {
+  uint32_t h = (x * kHashMul) >> shift;
+  while (true) {
+    const uint32_t k = keys[h];
+    if (k == x) return (int)pos[h];
+    if (k == kSentinel) return -1;
+    h = (h + 1) & mask;
+  }
+}
+
+// 4-cliques with lowest vertex u; `nthreads` threads (one warp or the CTA)
+// cooperate, separated by sync().  On entry and on return every key slot of
+// the hash holds kSentinel and the d * W row words are zero.
+template <typename Sync>
+__device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t *keys, uint32_t *pos,
+                                        uint32_t max_log, uint32_t *rows, uint32_t tid,
+                                        uint32_t nthreads, Sync sync) {
+  const int lane = tid & 31;
+  const uint2 ru = g.row[u];
+  const uint32_t d = ru.y;
+  const uint32_t *au = g.adj + (uint64_t)ru.x * 4;
+  const uint32_t W = (d + 31) >> 5;
+  int l = hash_log2(d);
+  if (l > (int)max_log) l = (int)max_log;
+  const uint32_t mask = (1u << l) - 1;
+  const int shift = 32 - l;
+  for (uint32_t i = tid; i < d; i += nthreads) pos_insert(keys, pos, mask, shift, au[i], i);
+  sync();
+  const uint32_t maxu = au[d - 1];
+  // rows: 32 rows per warp step, ids of each N+(v) walked flattened
+  for (uint32_t r0 = tid & ~31u; r0 < d; r0 += nthreads) {
+    const uint32_t i = r0 + lane;
+    uint32_t q4 = 0, e = 0;
+    if (i < d) {
+      const uint2 rv = g.row[au[i]];
+      q4 = rv.x;
+      e = prefix_below(g.adj + (uint64_t)rv.x * 4, rv.y, maxu + 1);  // ids <= max N+(u)
+    }
+    const uint32_t incl = warp_inclusive_sum(e, lane);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t shiftp = 0u - (incl - e);
+    for (uint32_t pb = 0; pb < total; pb += 32) {
+      const uint32_t p = pb + lane;
+      const int o = warp_owner(incl, p);
+      const uint32_t oq = __shfl_sync(kFull, q4, o);
+      const uint32_t os = __shfl_sync(kFull, shiftp, o);
+      if (p < total) {
+        const int j = pos_find(keys, pos, mask, shift, g.adj[(uint64_t)oq * 4 + (uint32_t)(os + p)]);
+        if (j >= 0) atomicOr(&rows[(r0 + o) * W + ((uint32_t)j >> 5)], 1u << (j & 31));
       }
     }
-    cls[u] = c;
-    costL[u] = cl;
-    kW[u] = kw;
-    kC[u] = kc;
   }
-}
-
-__global__ void k_split_tiles(const uint2 *__restrict__ row, uint32_t n,
-                              const uint32_t *__restrict__ off, Tile *__restrict__ tiles) {
-  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
-       u += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t kk = off[u + 1] - off[u];
-    if (!kk) continue;
-    const uint32_t span = row[u].y - 2;
-    for (uint32_t i = 0; i < kk; ++i) {
-      Tile t;
-      t.v0 = (uint32_t)u;
-      t.v1 = (uint32_t)u + 1;
-      t.j0 = (uint32_t)((uint64_t)i * span / kk);
-      t.j1 = (uint32_t)((uint64_t)(i + 1) * span / kk);
-      tiles[off[u] + i] = t;
+  sync();
+  // count: for every set bit (i, j), the common later positions of rows i and j
+  unsigned long long cnt = 0;
+  for (uint32_t it = tid; it < d * W; it += nthreads) {
+    const uint32_t i = it / W, w = it - i * W;
+    const uint32_t *ri = rows + i * W;
+    uint32_t bits = ri[w];
+    while (bits) {
+      const uint32_t j = w * 32 + (__ffs(bits) - 1);
+      bits &= bits - 1;
+      const uint32_t *rj = rows + j * W;
+      for (uint32_t ww = w; ww < W; ++ww) cnt += __popc(ri[ww] & rj[ww]);
     }
   }
+  sync();
+  for (uint32_t it = tid; it < d * W; it += nthreads) rows[it] = 0;
+  for (uint32_t h = tid; h <= mask; h += nthreads) keys[h] = kSentinel;
+  sync();
+  return cnt;
 }
 
-__global__ void k_group_tiles(const uint32_t *__restrict__ starts, uint64_t G, uint32_t L,
-                              Tile *__restrict__ tiles) {
-  for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G;
-       g += (uint64_t)gridDim.x * blockDim.x) {
-    Tile t;
-    t.v0 = starts[g];
-    t.v1 = g + 1 < G ? starts[g + 1] : L;
-    t.j0 = 0;
-    t.j1 = kGroupTile;
-    tiles[g] = t;
+__global__ void __launch_bounds__(kK4Threads, 1)
+    k_k4(GraphView g, const uint32_t *__restrict__ cta_list, uint32_t c_lo, uint32_t c_hi,
+         const uint32_t *__restrict__ warp_list, uint32_t w_lo, uint32_t w_hi,
+         uint32_t *__restrict__ pool, uint64_t pool_words, SchedState *sched,
+         unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  __shared__ uint32_t s_idx;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long cnt = 0;
+  // phase 1: CTA vertices, largest first
+  {
+    uint32_t *keys = sm, *pos = sm + (1u << kK4CtaLog), *srows = sm + 2 * (1u << kK4CtaLog);
+    for (uint32_t i = threadIdx.x; i < (1u << kK4CtaLog); i += blockDim.x) keys[i] = kSentinel;
+    for (uint32_t i = threadIdx.x; i < kK4CtaRowWords; i += blockDim.x) srows[i] = 0;
+    while (true) {
+      if (threadIdx.x == 0) s_idx = c_lo + atomicAdd(&sched->next_cta, 1u);
+      __syncthreads();
+      const uint32_t k = s_idx;
+      __syncthreads();  // every thread has read s_idx
+      if (k >= c_hi) break;
+      const uint32_t u = cta_list[k];
+      const uint32_t d = g.row[u].y;
+      const uint64_t words = (uint64_t)d * ((d + 31) >> 5);
+      uint32_t *rows = words <= kK4CtaRowWords ? srows : pool + (uint64_t)blockIdx.x * pool_words;
+      cnt += k4_vertex(g, u, keys, pos, kK4CtaLog, rows, threadIdx.x, blockDim.x,
+                       [] { __syncthreads(); });
+    }
   }
+  // phase 2: warp vertices, each warp in its own region of shared memory
+  uint32_t *keys = sm + warp * kK4WarpWords, *pos = keys + (1u << kK4WarpLog),
+           *rows = pos + (1u << kK4WarpLog);
+  for (uint32_t i = lane; i < (1u << kK4WarpLog); i += 32) keys[i] = kSentinel;
+  for (uint32_t i = lane; i < kK4WarpMaxD * (kK4WarpMaxD / 32); i += 32) rows[i] = 0;
+  __syncwarp();
+  while (true) {
+    uint32_t c = 0;
+    if (lane == 0) c = atomicAdd(&sched->next_warp, 32u);
+    c = __shfl_sync(kFull, c, 0);
+    const uint32_t i0 = w_lo + c;
+    if (i0 >= w_hi) break;
+    const uint32_t nb = min(32u, w_hi - i0);
+    const uint32_t myu = lane < nb ? warp_list[i0 + lane] : 0u;
+    for (uint32_t q = 0; q < nb; ++q)
+      cnt += k4_vertex(g, __shfl_sync(kFull, myu, q), keys, pos, kK4WarpLog, rows, lane, 32,
+                       [] { __syncwarp(); });
+  }
+  cnt = warp_sum_u64(cnt);
+  if (lane == 0 && cnt) atomicAdd(out, cnt);
 }
 
+// ---- plans ------------------------------------------------------------------
 struct ClassIs {
   const uint8_t *cls;
   uint8_t c;
   __host__ __device__ bool operator()(uint32_t v) const { return cls[v] == c; }
 };
-struct CostOf {
-  const uint64_t *cost;
-  __host__ __device__ uint64_t operator()(uint32_t v) const { return cost[v]; }
-};
-struct Target {
-  uint64_t tw;
-  __host__ __device__ uint64_t operator()(uint64_t g) const { return g * tw; }
-};
-
 // C4 per-vertex class by an upper bound of its wedge count.
 __global__ void k_c4_classify(const uint2 *__restrict__ srow, const uint32_t *__restrict__ sadj,
                               const uint32_t *__restrict__ dplus, uint32_t n, uint32_t warp_cap,
@@ -669,6 +592,15 @@ __global__ void k_c4_fill_tiles(const uint2 *__restrict__ srow, const uint32_t *
   }
 }
 
+struct DegIn {
+  const uint32_t *d;
+  uint32_t lo, hi;
+  __host__ __device__ bool operator()(uint32_t u) const { return d[u] >= lo && d[u] <= hi; }
+};
+struct DegOf {
+  const uint32_t *d;
+  __host__ __device__ uint32_t operator()(uint32_t u) const { return d[u]; }
+};
 struct AtMost {
   uint64_t cap;
   __host__ __device__ bool operator()(uint64_t w) const { return w <= cap; }
@@ -693,48 +625,32 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
   auto plan = std::make_unique<PatternPlan>();
   const uint32_t n = g->n;
   auto pol = thrust::cuda::par_nosync.on(s);
-  const uint64_t tw = 1u << 16, twc = 1u << 20;
-  DevBuf<uint8_t> cls;
-  DevBuf<uint64_t> costL;
-  DevBuf<uint32_t> kW, kC;
-  GARY_TRY(cls.alloc(n, s));
-  GARY_TRY(costL.alloc(n, s));
-  GARY_TRY(kW.alloc((uint64_t)n + 1, s));
-  GARY_TRY(kC.alloc((uint64_t)n + 1, s));
-  k_k4_classify<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, g->wedge.p, n, tw, twc, cls.p, costL.p,
-                                                 kW.p, kC.p);
-  GARY_CUDA(cudaGetLastError());
-  GARY_CUDA(cudaMemsetAsync(kW.p + n, 0, 4, s));
-  GARY_CUDA(cudaMemsetAsync(kC.p + n, 0, 4, s));
-  thrust::exclusive_scan(pol, kW.p, kW.p + n + 1, kW.p, 0u);
-  thrust::exclusive_scan(pol, kC.p, kC.p + n + 1, kC.p, 0u);
-  uint32_t nW = 0, nC = 0;
-  GARY_CUDA(cudaMemcpyAsync(&nW, kW.p + n, 4, cudaMemcpyDeviceToHost, s));
-  GARY_CUDA(cudaMemcpyAsync(&nC, kC.p + n, 4, cudaMemcpyDeviceToHost, s));
+  const uint32_t *dp = g->dag.outdeg.p;
+  // warp vertices (3 <= d+ <= 128) in id order; CTA vertices largest first
   GARY_TRY(plan->light.alloc_persistent(std::max<uint32_t>(n, 1)));
-  const uint32_t L = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
-                                                thrust::counting_iterator<uint32_t>(n), plan->light.p,
-                                                ClassIs{cls.p, kClassLight}) - plan->light.p);
-  DevBuf<uint64_t> lc;
-  GARY_TRY(lc.alloc((uint64_t)L + 1, s));
-  auto costs = thrust::make_transform_iterator(plan->light.p, CostOf{costL.p});
-  thrust::exclusive_scan(pol, costs, costs + L, lc.p, 0ull);
-  const uint64_t totalL = L ? thrust::reduce(pol, costs, costs + L, 0ull) : 0;
-  GARY_CUDA(cudaStreamSynchronize(s));
-  const uint64_t G = totalL ? (totalL + tw - 1) / tw : 0;
-  plan->n_cta = nC;
-  plan->n_warp = (uint32_t)(nW + G);
-  GARY_TRY(plan->tiles.alloc_persistent(std::max<uint64_t>((uint64_t)nC + nW + G, 1)));
-  k_split_tiles<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, n, kC.p, plan->tiles.p);
-  k_split_tiles<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, n, kW.p, plan->tiles.p + nC);
-  if (G) {
-    DevBuf<uint32_t> starts;
-    GARY_TRY(starts.alloc(G, s));
-    auto tg = thrust::make_transform_iterator(thrust::counting_iterator<uint64_t>(0), Target{tw});
-    thrust::lower_bound(pol, lc.p, lc.p + L, tg, tg + G, starts.p);
-    k_group_tiles<<<grid_for(G), kThreads, 0, s>>>(starts.p, G, L, plan->tiles.p + nC + nW);
+  plan->n_light = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                             thrust::counting_iterator<uint32_t>(n), plan->light.p,
+                                             DegIn{dp, 3, kK4WarpMaxD}) - plan->light.p);
+  GARY_TRY(plan->mid.alloc_persistent(std::max<uint32_t>(n, 1)));
+  plan->n_mid = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                           thrust::counting_iterator<uint32_t>(n), plan->mid.p,
+                                           DegIn{dp, kK4WarpMaxD + 1, 0xFFFFFFFFu}) - plan->mid.p);
+  if (plan->n_mid) {
+    DevBuf<uint32_t> key;
+    GARY_TRY(key.alloc(plan->n_mid, s));
+    thrust::transform(pol, plan->mid.p, plan->mid.p + plan->n_mid, key.p, DegOf{dp});
+    thrust::sort_by_key(pol, key.p, key.p + plan->n_mid, plan->mid.p, thrust::greater<uint32_t>());
+    uint32_t dmax = 0;
+    GARY_CUDA(cudaMemcpyAsync(&dmax, key.p, 4, cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaStreamSynchronize(s));
+    plan->max_pre = dmax;
+    plan->win_ctas = (uint32_t)sm_count();
+    const uint64_t words = (uint64_t)dmax * ((dmax + 31) / 32);
+    if (words > kK4CtaRowWords) {  // rows of the largest vertices live in HBM, one buffer per CTA
+      GARY_TRY(plan->cursors.alloc_persistent((uint64_t)plan->win_ctas * words));
+      GARY_CUDA(cudaMemsetAsync(plan->cursors.p, 0, plan->cursors.bytes(), s));
+    }
   }
-  GARY_CUDA(cudaGetLastError());
   GARY_TRY(plan->sched.alloc_persistent(1));
   GARY_CUDA(cudaStreamSynchronize(s));
   *out = plan.release();
@@ -743,28 +659,36 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
 
 int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaStream_t s,
               uint32_t shard, uint32_t nshards) {
-  const size_t smem = (size_t)2 * kCtaSlots * 4;  // >= kPWarps * 2 * kPSlots words
-  static_assert(2 * kCtaSlots >= kPWarps * 2 * kPSlots, "shared buffer too small for warp tables");
+  auto part = [&](uint32_t total, uint32_t k) { return (uint32_t)((uint64_t)total * k / nshards); };
+  const uint32_t c0 = part(plan->n_mid, shard), c1 = part(plan->n_mid, shard + 1);
+  const uint32_t w0 = part(plan->n_light, shard), w1 = part(plan->n_light, shard + 1);
+  const size_t smem = (size_t)kK4SmemWords * 4;
   static bool attr[64] = {false};
   const int dev = device_ordinal();
   if (dev < 64 && !attr[dev]) {
     GARY_CUDA(cudaFuncSetAttribute(k_k4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr[dev] = true;
   }
-  int per_sm = 0;
-  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_k4, kPWarps * 32, smem));
-  if (per_sm < 1) per_sm = 1;
-  const TileRange rng = shard_range(plan->n_cta, plan->n_warp, shard, nshards);
+  const uint64_t dmax = plan->max_pre;
+  const uint64_t pool_words = plan->cursors.p ? dmax * ((dmax + 31) / 32) : 0;
   GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
   GARY_CUDA(cudaMemsetAsync(d_out, 0, 8, s));
   GARY_CUDA(cudaEventRecord(g->ev0, s));
-  k_k4<<<(unsigned)(sm_count() * per_sm), kPWarps * 32, smem, s>>>(
-      g->view(), plan->tiles.p, plan->light.p, plan->n_cta, rng, plan->sched.p, d_out);
+  if (c1 > c0 || w1 > w0) {
+    // one CTA per SM; the pool holds one row buffer per CTA of the grid
+    const unsigned grid = (unsigned)sm_count();
+    if (plan->cursors.p && grid > plan->win_ctas) {
+      set_error("4-clique row pool sized for %u CTAs, grid has %u", plan->win_ctas, grid);
+      return GARY_ERR_INVALID;
+    }
+    k_k4<<<grid, kK4Threads, smem, s>>>(g->view(), plan->mid.p, c0, c1, plan->light.p, w0, w1,
+                                        plan->cursors.p, pool_words, plan->sched.p, d_out);
+  }
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
-  g->last.tiles = (rng.cta_hi - rng.cta_lo) + (rng.warp_hi - rng.warp_lo);
-  g->last.cta_tiles = rng.cta_hi - rng.cta_lo;
+  g->last.tiles = (c1 - c0) + (w1 - w0);
+  g->last.cta_tiles = c1 - c0;
   g->last_timed = true;
   return GARY_OK;
 }
