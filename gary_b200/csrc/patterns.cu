@@ -384,8 +384,8 @@ __device__ __forceinline__ int pos_find(const uint32_t *keys, const uint32_t *po
   uint32_t h = (x * kHashMul) >> shift;
   while (true) {
     const uint32_t k = keys[h];
+    if (k == kSentinel) return -1;  // first: x may itself be the padding value
     if (k == x) return (int)pos[h];
-    if (k == kSentinel) return -1;
     h = (h + 1) & mask;
   }
 }
@@ -409,26 +409,36 @@ __device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t
   for (uint32_t i = tid; i < d; i += nthreads) pos_insert(keys, pos, mask, shift, au[i], i);
   sync();
   const uint32_t maxu = au[d - 1];
-  // rows: 32 rows per warp step, ids of each N+(v) walked flattened
+  // rows: 32 rows per warp step.  Each N+(v) is read as 32-byte octets from
+  // its (32-byte aligned, padded) start up to the last id <= max N+(u); the
+  // lanes walk the 32 lists' octets flattened.  Ids past that point (larger
+  // ids, padding) are not in N+(u), so the hash rejects them: no mask.
+  const uint4 *adj4 = reinterpret_cast<const uint4 *>(g.adj);
+  auto mark = [&](uint32_t row, uint32_t x) {
+    const int j = pos_find(keys, pos, mask, shift, x);
+    if (j >= 0) atomicOr(&rows[row * W + ((uint32_t)j >> 5)], 1u << (j & 31));
+  };
   for (uint32_t r0 = tid & ~31u; r0 < d; r0 += nthreads) {
     const uint32_t i = r0 + lane;
-    uint32_t q4 = 0, e = 0;
+    uint32_t o0 = 0, no = 0;
     if (i < d) {
       const uint2 rv = g.row[au[i]];
-      q4 = rv.x;
-      e = prefix_below(g.adj + (uint64_t)rv.x * 4, rv.y, maxu + 1);  // ids <= max N+(u)
+      const uint32_t e = prefix_below(g.adj + (uint64_t)rv.x * 4, rv.y, maxu + 1);  // ids <= max N+(u)
+      o0 = rv.x >> 1;
+      no = (e + 7) >> 3;
     }
-    const uint32_t incl = warp_inclusive_sum(e, lane);
+    const uint32_t incl = warp_inclusive_sum(no, lane);
     const uint32_t total = __shfl_sync(kFull, incl, 31);
-    const uint32_t shiftp = 0u - (incl - e);
+    const uint32_t bias = o0 - (incl - no);
     for (uint32_t pb = 0; pb < total; pb += 32) {
       const uint32_t p = pb + lane;
       const int o = warp_owner(incl, p);
-      const uint32_t oq = __shfl_sync(kFull, q4, o);
-      const uint32_t os = __shfl_sync(kFull, shiftp, o);
+      const uint32_t oc = __shfl_sync(kFull, bias, o) + p;
       if (p < total) {
-        const int j = pos_find(keys, pos, mask, shift, g.adj[(uint64_t)oq * 4 + (uint32_t)(os + p)]);
-        if (j >= 0) atomicOr(&rows[(r0 + o) * W + ((uint32_t)j >> 5)], 1u << (j & 31));
+        const uint4 a = adj4[2 * (uint64_t)oc], b = adj4[2 * (uint64_t)oc + 1];
+        const uint32_t row = r0 + o;
+        mark(row, a.x); mark(row, a.y); mark(row, a.z); mark(row, a.w);
+        mark(row, b.x); mark(row, b.y); mark(row, b.z); mark(row, b.w);
       }
     }
   }
