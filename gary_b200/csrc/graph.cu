@@ -7,6 +7,7 @@
 #include <thrust/execution_policy.h>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/reverse_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 #include <thrust/reduce.h>
 #include <thrust/remove.h>
 #include <thrust/scan.h>
@@ -17,6 +18,7 @@
 #include <algorithm>
 #include <exception>
 #include <new>
+#include <vector>
 
 #include "graph.cuh"
 
@@ -146,6 +148,187 @@ __global__ void k_make_keys(const uint32_t *__restrict__ rowid, const uint32_t *
     keys[e] = ((uint64_t)s << lg) | t;
   }
 }
+
+// Ranked DAG without a global sort.  Pass 1 validates every CSR entry and
+// counts the kept ones per ranked row (the row of the entry's earlier
+// endpoint); pass 2 writes each kept entry's later endpoint into its row at
+// an atomically claimed slot; a segmented sort then orders every row.
+// Symmetric input keeps the copy stored in the earlier endpoint's row; `dag`
+// input keeps every entry.
+__device__ __forceinline__ bool kept_entry(uint32_t a, uint32_t b, const uint32_t *__restrict__ deg,
+                                           bool dag, uint32_t &s, uint32_t &t) {
+  const bool fwd = before(a, b, deg);
+  if (!fwd && !dag) return false;
+  s = fwd ? a : b;
+  t = fwd ? b : a;
+  return true;
+}
+
+__global__ void k_count_rows(const uint32_t *__restrict__ rowid, const uint32_t *__restrict__ idx,
+                             uint64_t nnz, uint32_t n, const uint32_t *__restrict__ deg,
+                             const uint32_t *__restrict__ rank, bool dag, bool validate,
+                             uint32_t *__restrict__ dplus, unsigned long long *__restrict__ kept,
+                             unsigned *err) {
+  unsigned long long mine = 0;
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < nnz;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t a = rowid[e], b = idx[e];
+    if (b >= n) {
+      atomicOr(err, kErrRange);
+      continue;
+    }
+    if (a == b) {
+      atomicOr(err, kErrLoop);
+      continue;
+    }
+    if (validate && e + 1 < nnz && rowid[e + 1] == a && idx[e + 1] <= b) atomicOr(err, kErrOrder);
+    uint32_t su, tv;
+    if (!kept_entry(a, b, deg, dag, su, tv)) continue;
+    atomicAdd(&dplus[rank[su]], 1u);
+    ++mine;
+  }
+  for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(kFull, mine, o);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(kept, mine);
+}
+
+__global__ void k_fill_rows(const uint32_t *__restrict__ rowid, const uint32_t *__restrict__ idx,
+                            uint64_t nnz, uint32_t n, const uint32_t *__restrict__ deg,
+                            const uint32_t *__restrict__ rank, bool dag, const uint2 *__restrict__ row,
+                            uint32_t *__restrict__ cursor, uint32_t *__restrict__ adj) {
+  for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < nnz;
+       e += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t a = rowid[e], b = idx[e];
+    if (b >= n || a == b) continue;
+    uint32_t su, tv;
+    if (!kept_entry(a, b, deg, dag, su, tv)) continue;
+    const uint32_t r = rank[su];
+    const uint32_t slot = atomicAdd(&cursor[r], 1u);
+    adj[(uint64_t)row[r].x * 4 + slot] = rank[tv];
+  }
+}
+
+// plen4[u] = quads of u's padded list (whole octets)
+__global__ void k_octet_quads(const uint32_t *__restrict__ dplus, uint32_t n, uint64_t *__restrict__ plen4) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
+       u += (uint64_t)gridDim.x * blockDim.x)
+    plen4[u] = ((dplus[u] + 7u) >> 3) << 1;
+}
+
+// A sorted row holding the same id twice: a duplicate edge in the input.
+// Also wedge[u] = sum of d+(v) over v in N+(u); one warp per row.
+__global__ void k_rows_check_wedges(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
+                                    uint32_t n, unsigned long long *__restrict__ wedge,
+                                    unsigned *err) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
+    const uint2 r = row[u];
+    const uint32_t *l = adj + (uint64_t)r.x * 4;
+    unsigned long long w = 0;
+    bool dup = false;
+    for (uint32_t k = lane; k < r.y; k += 32) {
+      const uint32_t x = l[k];
+      w += row[x].y;
+      dup |= k + 1 < r.y && l[k + 1] == x;
+    }
+    for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(kFull, w, o);
+    if (__any_sync(kFull, dup) && lane == 0) atomicOr(err, kErrDup);
+    if (lane == 0) wedge[u] = w;
+  }
+}
+
+// ---- sorting the rows of a padded CSR in place ----------------------------
+// Rows of up to 32 ids: a warp ranks its lane values (ties by lane, so equal
+// ids stay adjacent and a duplicate check still sees them).  Rows of up to
+// kSortWarpMax ids: a warp bitonic-sorts them in its shared-memory slice.
+// Longer rows: a CTA bitonic sort up to kSortCtaMax ids; rarer longer ones
+// go to a library segmented sort.
+constexpr uint32_t kSortWarps = 8;
+constexpr uint32_t kSortWarpMax = 1024;
+constexpr uint32_t kSortCtaMax = 8192;
+
+template <typename Sync>
+__device__ __forceinline__ void bitonic_smem(uint32_t *a, uint32_t P, uint32_t tid, uint32_t nth, Sync sync) {
+  for (uint32_t k = 2; k <= P; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = tid; i < P; i += nth) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const uint32_t x = a[i], y = a[l];
+          const bool up = (i & k) == 0;
+          if ((x > y) == up) {
+            a[i] = y;
+            a[l] = x;
+          }
+        }
+      }
+      sync();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSortWarps * 32)
+    k_sort_rows_warp(const uint2 *__restrict__ row, uint32_t n, uint32_t *__restrict__ adj) {
+  __shared__ uint32_t buf[kSortWarps * kSortWarpMax];
+  const int lane = threadIdx.x & 31;
+  uint32_t *a = buf + (threadIdx.x >> 5) * kSortWarpMax;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
+    const uint2 r = row[u];
+    const uint32_t d = r.y;
+    if (d < 2 || d > kSortWarpMax) continue;
+    uint32_t *l = adj + (uint64_t)r.x * 4;
+    if (d <= 32) {
+      const uint32_t x = (uint32_t)lane < d ? l[lane] : kSentinel;
+      uint32_t rk = 0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const uint32_t y = __shfl_sync(kFull, x, j);
+        rk += (y < x) || (y == x && j < lane);
+      }
+      __syncwarp();
+      if ((uint32_t)lane < d) l[rk] = x;
+      __syncwarp();
+      continue;
+    }
+    uint32_t P = 64;
+    while (P < d) P <<= 1;
+    for (uint32_t i = lane; i < P; i += 32) a[i] = i < d ? l[i] : kSentinel;
+    __syncwarp();
+    bitonic_smem(a, P, lane, 32, [] { __syncwarp(); });
+    for (uint32_t i = lane; i < d; i += 32) l[i] = a[i];
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(512)
+    k_sort_rows_cta(const uint2 *__restrict__ row, const uint32_t *__restrict__ list, uint32_t nl,
+                    uint32_t *__restrict__ adj) {
+  __shared__ uint32_t a[kSortCtaMax];
+  for (uint32_t k = blockIdx.x; k < nl; k += gridDim.x) {
+    const uint2 r = row[list[k]];
+    const uint32_t d = r.y;
+    uint32_t *l = adj + (uint64_t)r.x * 4;
+    uint32_t P = 1024;
+    while (P < d) P <<= 1;
+    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) a[i] = i < d ? l[i] : kSentinel;
+    __syncthreads();
+    bitonic_smem(a, P, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x) l[i] = a[i];
+    __syncthreads();
+  }
+}
+
+struct RowLenIn {
+  const uint2 *row;
+  uint32_t lo, hi;
+  __host__ __device__ bool operator()(uint32_t u) const { return row[u].y > lo && row[u].y <= hi; }
+};
+struct RowOf {
+  const uint2 *row;
+  __host__ __device__ uint2 operator()(uint32_t u) const { return row[u]; }
+};
+
 
 __global__ void k_check_unique(const uint64_t *__restrict__ keys, uint64_t m, unsigned *err) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i + 1 < m;
@@ -342,6 +525,117 @@ int padded_from_keys(const DevBuf<uint64_t> &keys, uint64_t m, uint32_t n, int l
   return GARY_OK;
 }
 
+// The ranked DAG's padded lists straight from the CSR entries (count, fill,
+// segmented sort; no sort of all edges), plus per-vertex wedge counts.
+int ranked_dag_by_rows(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz, uint32_t n,
+                       const uint32_t *deg, const uint32_t *rank, bool dag, bool validate,
+                       unsigned *err, PaddedCSR &c, DevBuf<uint64_t> &wedge, uint64_t &m,
+                       cudaStream_t s) {
+  auto pol = thrust::cuda::par_nosync.on(s);
+  PhaseTrace tr("dag rows", s);
+  c.n = n;
+  GARY_TRY(c.outdeg.alloc_persistent(n));
+  GARY_CUDA(cudaMemsetAsync(c.outdeg.p, 0, (uint64_t)n * 4, s));
+  DevBuf<unsigned long long> dkept;
+  GARY_TRY(dkept.alloc(1, s));
+  GARY_CUDA(cudaMemsetAsync(dkept.p, 0, 8, s));
+  if (nnz)
+    k_count_rows<<<grid_for(nnz), kThreads, 0, s>>>(rowid, didx, nnz, n, deg, rank, dag, validate,
+                                                    c.outdeg.p, dkept.p, err);
+  GARY_CUDA(cudaGetLastError());
+  DevBuf<uint64_t> off4;
+  GARY_TRY(off4.alloc((uint64_t)n + 1, s));
+  k_octet_quads<<<grid_for(n), kThreads, 0, s>>>(c.outdeg.p, n, off4.p);
+  GARY_CUDA(cudaMemsetAsync(off4.p + n, 0, 8, s));
+  thrust::exclusive_scan(pol, off4.p, off4.p + n + 1, off4.p, 0ull);
+  uint64_t quads = 0;
+  unsigned long long km = 0;
+  unsigned herr = 0;
+  tr.mark("count");
+  GARY_CUDA(cudaMemcpyAsync(&quads, off4.p + n, 8, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaMemcpyAsync(&km, dkept.p, 8, cudaMemcpyDeviceToHost, s));
+  GARY_TRY(read_err(err, s, &herr));
+  if (herr) return input_error(herr);
+  m = km;
+  c.m = m;
+  if (!dag && 2 * m != nnz) return input_error(kErrAsym);
+  if (quads >= (1ull << 32)) {
+    set_error("graph too large: %llu padded words", (unsigned long long)quads * 4);
+    return GARY_ERR_UNSUPPORTED;
+  }
+  c.words = quads * 4;
+  GARY_TRY(c.adj.alloc_persistent(c.words + 4));
+  GARY_CUDA(cudaMemsetAsync(c.adj.p, 0xFF, c.adj.bytes(), s));
+  GARY_TRY(c.row.alloc_persistent(n));
+  GARY_TRY(c.indptr.alloc_persistent((uint64_t)n + 1));
+  k_row_records<<<grid_for((uint64_t)n + 1), kThreads, 0, s>>>(off4.p, c.outdeg.p, n, c.row.p,
+                                                              c.indptr.p);
+  GARY_CUDA(cudaGetLastError());
+  off4.release();
+  tr.mark("allocate + records");
+  {
+    DevBuf<uint32_t> cursor;
+    GARY_TRY(cursor.alloc(n, s));
+    GARY_CUDA(cudaMemsetAsync(cursor.p, 0, (uint64_t)n * 4, s));
+    if (nnz)
+      k_fill_rows<<<grid_for(nnz), kThreads, 0, s>>>(rowid, didx, nnz, n, deg, rank, dag, c.row.p,
+                                                     cursor.p, c.adj.p);
+    GARY_CUDA(cudaGetLastError());
+  }
+  tr.mark("fill");
+  // order every row in place
+  if (m) {
+    k_sort_rows_warp<<<sm_count() * 8, kSortWarps * 32, 0, s>>>(c.row.p, n, c.adj.p);
+    GARY_CUDA(cudaGetLastError());
+    DevBuf<uint32_t> big;
+    GARY_TRY(big.alloc(std::max<uint32_t>(n, 1), s));
+    const uint32_t nb = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                                   thrust::counting_iterator<uint32_t>(n), big.p,
+                                                   RowLenIn{c.row.p, kSortWarpMax, kSortCtaMax}) - big.p);
+    if (nb) {
+      k_sort_rows_cta<<<std::min<uint32_t>(nb, sm_count() * 4), 512, 0, s>>>(c.row.p, big.p, nb, c.adj.p);
+      GARY_CUDA(cudaGetLastError());
+    }
+    const uint32_t nh = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                                   thrust::counting_iterator<uint32_t>(n), big.p,
+                                                   RowLenIn{c.row.p, kSortCtaMax, 0xFFFFFFFFu}) - big.p);
+    if (nh) {  // the longest rows (rare; d+ above 8192): one library radix sort per row
+      std::vector<uint32_t> hl(nh);
+      std::vector<uint2> hr(nh);
+      DevBuf<uint2> rr;
+      GARY_TRY(rr.alloc(nh, s));
+      thrust::transform(pol, big.p, big.p + nh, rr.p, RowOf{c.row.p});
+      GARY_CUDA(cudaMemcpyAsync(hr.data(), rr.p, (uint64_t)nh * 8, cudaMemcpyDeviceToHost, s));
+      GARY_CUDA(cudaStreamSynchronize(s));
+      uint32_t dmax = 0;
+      for (const uint2 &r : hr) dmax = std::max(dmax, r.y);
+      DevBuf<uint32_t> tmpk;
+      GARY_TRY(tmpk.alloc(dmax, s));
+      size_t tmp = 0;
+      GARY_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, c.adj.p, tmpk.p, (int)dmax, 0, 32, s));
+      DevBuf<uint8_t> t;
+      GARY_TRY(t.alloc(std::max<size_t>(tmp, 1), s));
+      for (const uint2 &r : hr) {
+        uint32_t *l = c.adj.p + (uint64_t)r.x * 4;
+        size_t tb = tmp;
+        GARY_CUDA(cub::DeviceRadixSort::SortKeys(t.p, tb, l, tmpk.p, (int)r.y, 0, 32, s));
+        GARY_CUDA(cudaMemcpyAsync(l, tmpk.p, (uint64_t)r.y * 4, cudaMemcpyDeviceToDevice, s));
+      }
+    }
+  }
+  tr.mark("row sort");
+  GARY_TRY(wedge.alloc_persistent(n));
+  k_rows_check_wedges<<<grid_for((uint64_t)n * 32), kThreads, 0, s>>>(
+      c.row.p, c.adj.p, n, reinterpret_cast<unsigned long long *>(wedge.p), err);
+  GARY_CUDA(cudaGetLastError());
+  if (validate || dag) {
+    GARY_TRY(read_err(err, s, &herr));
+    if (herr) return input_error(herr);
+  }
+  c.max_len = thrust::reduce(pol, c.outdeg.p, c.outdeg.p + n, 0u, MaxU32());
+  return GARY_OK;
+}
+
 // Oriented keys of every CSR entry, compacted and sorted.  rank == nullptr:
 // caller ids; else degree ranks.
 int oriented_keys(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz, uint32_t n,
@@ -516,39 +810,21 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   }
 
   tr.mark("row ids");
-  // 5. oriented, ranked keys: sorted, validated
-  DevBuf<uint64_t> keys;
+  // 5. the ranked DAG's padded lists, validated; per-vertex wedge counts
   uint64_t m = 0;
-  GARY_TRY(oriented_keys(rowid.p, didx, nnz, n, deg.p, rank.p, lg, dag, validate, err.p, keys, m, s));
-  unsigned herr = 0;
-  GARY_TRY(read_err(err.p, s, &herr));
-  if (herr) return input_error(herr);
-  if (!dag && 2 * m != nnz) return input_error(kErrAsym);
-  if (validate || dag) {
-    if (m > 1) k_check_unique<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, err.p);
-    GARY_TRY(read_err(err.p, s, &herr));
-    if (herr) return input_error(herr);
-  }
-
-  tr.mark("oriented keys + sort");
-  // 6. the kernels' padded lists, per-vertex wedge counts, statistics
-  GARY_TRY(padded_from_keys(keys, m, n, lg, g->dag, s));
-  tr.mark("padded lists");
-  GARY_TRY(g->wedge.alloc_persistent(n));
-  GARY_CUDA(cudaMemsetAsync(g->wedge.p, 0, (uint64_t)n * 8, s));
-  if (m)
-    k_wedges<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, g->dag.outdeg.p,
-                                              reinterpret_cast<unsigned long long *>(g->wedge.p));
-  GARY_CUDA(cudaGetLastError());
+  GARY_TRY(ranked_dag_by_rows(rowid.p, didx, nnz, n, deg.p, rank.p, dag, validate, err.p, g->dag,
+                              g->wedge, m, s));
+  tr.mark("rows: count, fill, sort");
+  // 6. statistics
   g->out_deg_sq = thrust::transform_reduce(pol, g->dag.outdeg.p, g->dag.outdeg.p + n, Sq(), 0ull,
                                            thrust::plus<uint64_t>());
   g->wedges = thrust::reduce(pol, g->wedge.p, g->wedge.p + n, 0ull);
   g->alg_bytes = 4 * g->out_deg_sq + 4 * g->wedges + 24 * m;
-  keys.release();
-  tr.mark("wedges + statistics");
+  tr.mark("statistics");
 
   // 7. the same orientation in caller ids, for the views (GARY_KEEP_IDS)
   if (keep_ids) {
+    DevBuf<uint64_t> keys;
     uint64_t m2 = 0;
     GARY_TRY(oriented_keys(rowid.p, didx, nnz, n, deg.p, nullptr, lg, dag, false, err.p, keys, m2, s));
     GARY_TRY(padded_from_keys(keys, m2, n, lg, g->kept, s));

@@ -247,3 +247,22 @@ def test_scratch_pool_setting_keeps_results(cuda):
                 assert g.count() == want
     finally:
         _lib.check(L.gary_tune(b"pool_keep_bytes", (1 << 64) - 1), "gary_tune")
+
+
+@pytest.mark.parametrize("k", [33, 1500, 9000])
+def test_complete_graph_long_rows(cuda, k):
+    """K_k: C(k,3) triangles.  Its oriented rows hold up to k-1 ids, so the
+    upload's row sort takes every path: warp ranks (<= 32), warp bitonic
+    (<= 1024), CTA bitonic (<= 8192) and the per-row library sort beyond."""
+    from math import comb
+
+    ptr = (np.arange(k + 1, dtype=np.uint64) * (k - 1))
+    full = np.tile(np.arange(k, dtype=np.uint32), k).reshape(k, k)
+    idx = full[~np.eye(k, dtype=bool)].astype(np.uint32)
+    with _upload_host(ptr, idx, k, _lib.GARY_VALIDATE) as g:
+        assert g.count() == comb(k, 3)
+        dp, di, _ = g.download()
+        assert np.all(np.diff(dp.astype(np.int64)) == np.arange(k - 1, -1, -1))
+        for u in (0, k // 2, k - 2):
+            row = di[dp[u]:dp[u + 1]]
+            assert np.array_equal(row, np.arange(u + 1, k, dtype=np.uint32))
