@@ -246,3 +246,51 @@ def gen_rmat_device(scale: int, seed: int, count: int, first: int = 0, stream=No
     check(load().gary_gen_rmat_device(scale, seed, first, count, src.data_ptr(), dst.data_ptr(),
                                       _stream(stream)), "gary_gen_rmat_device")
     return src, dst
+
+
+# ---- the reference's graph binaries (cereal binary archive layout) --------
+GARY_BIN_CSR = 0
+GARY_BIN_COO = 1
+
+
+def bin_info(path) -> tuple[int, int, int]:
+    """(format, n, nnz) of a graph binary written by the reference's
+    saveToBinary (format GARY_BIN_CSR or GARY_BIN_COO)."""
+    fmt, n, nnz = C.c_uint32(), C.c_uint32(), C.c_uint64()
+    check(load().gary_bin_info(str(path).encode(), C.byref(fmt), C.byref(n), C.byref(nnz)), "gary_bin_info")
+    return fmt.value, n.value, nnz.value
+
+
+def read_bin_csr(path) -> tuple[np.ndarray, np.ndarray]:
+    """(ptr uint64[n+1], idx uint32[nnz]) of a CSR graph binary, e.g. the
+    reference's csr_dag.bin (loadFromBinary<GraphCSR>)."""
+    fmt, n, nnz = bin_info(path)
+    if fmt != GARY_BIN_CSR:
+        raise GaryError(-4, f"{path} holds a COO graph, not a CSR")
+    ptr = np.empty(n + 1, np.uint64)
+    idx = np.empty(max(nnz, 1), np.uint32)
+    check(load().gary_bin_read_csr(str(path).encode(), ptr.ctypes.data, idx.ctypes.data), "gary_bin_read_csr")
+    return ptr, idx[:nnz]
+
+
+def read_bin_coo(path) -> tuple[int, np.ndarray, np.ndarray]:
+    """(n, src, dst) of a COO graph binary (loadFromBinary<GraphCOO>)."""
+    fmt, n, nnz = bin_info(path)
+    if fmt != GARY_BIN_COO:
+        raise GaryError(-4, f"{path} holds a CSR graph, not a COO")
+    src = np.empty(max(nnz, 1), np.uint32)
+    dst = np.empty(max(nnz, 1), np.uint32)
+    check(load().gary_bin_read_coo(str(path).encode(), src.ctypes.data, dst.ctypes.data), "gary_bin_read_coo")
+    return n, src[:nnz], dst[:nnz]
+
+
+def write_bin_csr(path, ptr, idx) -> None:
+    """Write a CSR graph binary in the reference's layout (saveToBinary)."""
+    ptr = np.ascontiguousarray(ptr, np.uint64)
+    idx = np.ascontiguousarray(idx, np.uint32)
+    n = len(ptr) - 1
+    check(load().gary_bin_write_csr(str(path).encode(), ptr.ctypes.data, idx.ctypes.data if len(idx) else None,
+                                    n, int(ptr[-1])), "gary_bin_write_csr")
+
+
+__all__ += ["bin_info", "read_bin_csr", "read_bin_coo", "write_bin_csr", "GARY_BIN_CSR", "GARY_BIN_COO"]

@@ -133,6 +133,10 @@ SIGNATURES = {
     "gary_csr_device_ptrs": (_INT, [_P, C.POINTER(_P), C.POINTER(_P)]),
     "gary_csr_download": (_INT, [_P, _P, _P]),
     "gary_csr_free": (_INT, [_P]),
+    "gary_bin_info": (_INT, [C.c_char_p, _P, _P, _P]),
+    "gary_bin_read_csr": (_INT, [C.c_char_p, _P, _P]),
+    "gary_bin_read_coo": (_INT, [C.c_char_p, _P, _P]),
+    "gary_bin_write_csr": (_INT, [C.c_char_p, _P, _P, _U32, _U64]),
     "gary_gen_er": (_INT, [_U32, _U64, _U64, _P, _P]),
     "gary_gen_rmat": (_INT, [_INT, _U64, _U64, _U64, _P, _P]),
     "gary_gen_rmat_device": (_INT, [_INT, _U64, _U64, _U64, _P, _P, _P]),

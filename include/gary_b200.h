@@ -316,6 +316,28 @@ int gary_csr_device_ptrs(const gary_csr *c, const uint64_t **ptr, const uint32_t
 int gary_csr_download(const gary_csr *c, uint64_t *ptr, uint32_t *idx);
 int gary_csr_free(gary_csr *c);
 
+/* ---- the reference's graph binaries (host only, no device use) -------- *
+ * Read and write the files the reference saves with cereal's binary archive
+ * (GraphCSR / GraphCOO save/load, include/Graph.h:132-148, 269-285; the
+ * loadFromBinary / saveToBinary pair, include/Graph.h:300-316; e.g. the
+ * csr_dag.bin its tests load, test/TriQueryTest.cu:51).  Layout, little-endian:
+ * uint32 version (1), uint32 format (0 CSR, 1 COO), int32 m, int64 nnz, then
+ * each array as a cereal shared pointer (uint32 id 0x8000000k) holding a
+ * uint64 count and the elements: CSR ptr (int64, m+1), idx (int32, nnz),
+ * deg (int32, m); COO row and col (int32, nnz each).
+ * gary_bin_info reports the format and sizes; the readers fill caller
+ * buffers of those sizes (ptr: n+1 words, idx: nnz; src/dst: nnz each) and
+ * check that the arrays agree; gary_bin_write_csr writes the CSR record,
+ * deriving deg from ptr.  Errors: GARY_ERR_INPUT for unreadable, truncated or
+ * inconsistent files. */
+#define GARY_BIN_CSR 0u
+#define GARY_BIN_COO 1u
+int gary_bin_info(const char *path, uint32_t *format, uint32_t *n, uint64_t *nnz);
+int gary_bin_read_csr(const char *path, uint64_t *ptr, uint32_t *idx);
+int gary_bin_read_coo(const char *path, uint32_t *src, uint32_t *dst);
+int gary_bin_write_csr(const char *path, const uint64_t *ptr, const uint32_t *idx, uint32_t n,
+                       uint64_t nnz);
+
 /* ---- seeded synthetic generators (host; RMAT also on the device) ------ *
  * Counter-based: edge i depends only on (seed, i), so any range can be
  * regenerated on the host to check a device batch. */

@@ -15,10 +15,12 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <memory>
 #include <random>
 #include <vector>
 
+#include "gary/Graph.h"
 #include "gary/kernels/GraphQueryHom.cuh"
 #include "gary/ops/Intersection.cuh"
 #include "gary/ops/Search.cuh"
@@ -125,9 +127,21 @@ int main(int argc, char **argv) {
   }
   const uint64_t want = cpu_count(*dag);
 
-  // ---- the reference's launch pattern over the shim views
+  // ---- the reference's file round trip (saveToBinary / loadFromBinary) and
+  // launch pattern over the shim views
+  const std::string bin = std::string(std::getenv("TMPDIR") ? std::getenv("TMPDIR") : "/tmp") +
+                          "/gary_shim_csr_dag_" + std::to_string(seed) + ".bin";
+  {
+    std::vector<eidT> p64(dag->ptr.begin(), dag->ptr.end());
+    std::vector<vidT> i32(dag->idx.begin(), dag->idx.end());
+    saveToBinary(GraphCSR(std::move(p64), std::move(i32)), bin);
+  }
+  auto loaded = loadFromBinary<GraphCSR>(bin);
+  std::remove(bin.c_str());
+  bool file_ok = loaded.numV() == (vidT)n && loaded.numE() == (eidT)dag->idx.size();
+  for (size_t k = 0; file_ok && k < dag->idx.size(); ++k) file_ok = loaded.getIdx()[k] == (vidT)dag->idx[k];
   DeviceGraphCtx ctx;
-  ctx.loadFromHost(dag);
+  ctx.loadFromHost(std::make_shared<GraphCSR>(std::move(loaded)));
   ctx.populateDevice();
   const DeviceGraph dg = ctx.getDeviceGraph();
   size_t *d_count;
@@ -159,7 +173,7 @@ int main(int argc, char **argv) {
   std::vector<uint64_t> hp;
   std::vector<uint32_t> hi;
   ctx.getHostCSR(hp, hi);
-  bool views_ok = hp.size() == (size_t)n + 1 && hi.size() == dag->idx.size() &&
+  bool views_ok = file_ok && hp.size() == (size_t)n + 1 && hi.size() == dag->idx.size() &&
                   dg.csr.numE() == dg.coo.numE() && dg.coo.numE() == hi.size() &&
                   ((uintptr_t)dg.csr.colIdx & 15) == 0;
 
