@@ -122,6 +122,7 @@ SIGNATURES = {
     "gary_tc_features": (_INT, [_P, _P, _P, _P]),
     "gary_tc_profile": (_INT, [_P, _INT, _P, _P, _P]),
     "gary_intersect_batch": (_INT, [_U64, _P, _P, _P, _P, _P, _P, _INT, _P, _P, _P, _P, _P, _P]),
+    "gary_intersect_num_batch": (_INT, [_U64, _P, _P, _P, _P, _P, _P, _INT, _P, _P, _P, _P, _P, _P, _P]),
     "gary_search_batch": (_INT, [_P, _U64, _P, _U64, _U32, _P, _P, _P]),
     "gary_zipf_table": (_INT, [_U32, C.c_double, _P]),
     "gary_gen_pair_host": (_INT, [_U64, _U64, _U32, _P, C.c_double, _U64, _P, _P, _P, _P]),

@@ -7,6 +7,10 @@
 //                         lists -- intersectBinarySearch (Intersection.cuh:18-135)
 //                         and the merge / bitmap paths the reference stubs out
 //                         (intersectMerge returns 0, Intersection.cuh:172-180)
+//   gary_intersect_num_batch  the same counts restricted to members below a
+//                         per-pair bound and outside a per-pair list of
+//                         excluded ids -- the intersect_num family the
+//                         reference leaves commented out (Intersection.cuh:361-485)
 //
 // Pair work is handed to warps by a persistent queue (32 pairs per grab).
 // Variants:
@@ -39,6 +43,26 @@ struct PairView {
   const uint32_t *a_len, *b_len;
   const uint32_t *a, *b;
 };
+
+// Bounded / ancestor-filtered counts (the reference's intersect_num family,
+// Intersection.cuh:361-485, left commented out there): per pair an exclusive
+// upper bound on the members and a list of excluded ids.
+struct PairFilter {
+  const uint32_t *bound;   // per pair, or null
+  const uint64_t *ex_off;  // per pair offsets into ex (npairs + 1), or null
+  const uint32_t *ex;
+};
+
+// first index in [0, len) with l[i] >= x (all lanes compute the same answer)
+__device__ __forceinline__ uint32_t so_lower_bound(const uint32_t *l, uint32_t len, uint32_t x) {
+  uint32_t b = 0, e = len;
+  while (b < e) {
+    const uint32_t m = (b + e) >> 1;
+    if (l[m] < x) b = m + 1;
+    else e = m;
+  }
+  return b;
+}
 
 struct PairOut {
   uint64_t *counts;        // per pair, or null
@@ -144,7 +168,7 @@ __device__ uint32_t pair_bitmap(const uint32_t *S, uint32_t ls, const uint32_t *
 }
 
 __global__ void __launch_bounds__(kSoWarps * 32)
-    k_intersect_pairs(PairView pv, uint64_t npairs, int variant, PairOut po,
+    k_intersect_pairs(PairView pv, uint64_t npairs, int variant, PairOut po, PairFilter pf,
                       unsigned long long *queue, unsigned long long *total) {
   __shared__ __align__(16) uint32_t smem[kSoWarps * kSoWarpWords];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -160,8 +184,13 @@ __global__ void __launch_bounds__(kSoWarps * 32)
     if (p0 >= npairs) break;
     const uint64_t pend = p0 + 32 < npairs ? p0 + 32 : npairs;
     for (uint64_t p = p0; p < pend; ++p) {
-      const uint32_t la = pv.a_len[p], lb = pv.b_len[p];
+      uint32_t la = pv.a_len[p], lb = pv.b_len[p];
       const uint32_t *A = pv.a + pv.a_off[p], *B = pv.b + pv.b_off[p];
+      const uint32_t bound = pf.bound ? pf.bound[p] : kInf;
+      if (pf.bound) {  // members < bound only: both lists end at the bound
+        la = so_lower_bound(A, la, bound);
+        lb = so_lower_bound(B, lb, bound);
+      }
       uint32_t *out = po.out_off ? po.out + po.out_off[p] : nullptr;
       uint32_t c2 = 0;
       if (la && lb) {
@@ -179,6 +208,21 @@ __global__ void __launch_bounds__(kSoWarps * 32)
         else {
           c2 = pair_bitmap(S, ls, L, ll, mine, out, lane);
         }
+      }
+      if (pf.ex_off && la && lb) {  // excluded ids that are members (each id once)
+        const uint64_t e0 = pf.ex_off[p], e1 = pf.ex_off[p + 1];
+        uint32_t drop = 0;
+        for (uint64_t k = e0 + lane; k < e1; k += 32) {
+          const uint32_t x = pf.ex[k];
+          bool first = x < bound;
+          for (uint64_t j = e0; first && j < k; ++j) first = pf.ex[j] != x;
+          if (first) {
+            const uint32_t ia = so_lower_bound(A, la, x), ib = so_lower_bound(B, lb, x);
+            drop += ia < la && A[ia] == x && ib < lb && B[ib] == x;
+          }
+        }
+        for (int o = 16; o; o >>= 1) drop += __shfl_xor_sync(kFull, drop, o);
+        c2 -= drop;
       }
       if (lane == 0 && po.counts) po.counts[p] = c2;
       local += c2;
@@ -355,8 +399,36 @@ extern "C" int gary_intersect_batch(uint64_t npairs, const uint64_t *d_a_off, co
   const PairView pv{d_a_off, d_b_off, d_a_len, d_b_len, d_a, d_b};
   const PairOut po{d_counts, d_out_off, d_out};
   k_intersect_pairs<<<(unsigned)(sm_count() * per_sm), kSoWarps * 32, 0, s>>>(
-      pv, npairs, variant, po, reinterpret_cast<unsigned long long *>(d_queue),
-      reinterpret_cast<unsigned long long *>(d_total));
+      pv, npairs, variant, po, PairFilter{nullptr, nullptr, nullptr},
+      reinterpret_cast<unsigned long long *>(d_queue), reinterpret_cast<unsigned long long *>(d_total));
+  GARY_CUDA(cudaGetLastError());
+  return GARY_OK;
+}
+
+extern "C" int gary_intersect_num_batch(uint64_t npairs, const uint64_t *d_a_off, const uint32_t *d_a_len,
+                                        const uint32_t *d_a, const uint64_t *d_b_off,
+                                        const uint32_t *d_b_len, const uint32_t *d_b, int variant,
+                                        const uint32_t *d_bound, const uint64_t *d_ex_off,
+                                        const uint32_t *d_ex, uint64_t *d_counts, uint64_t *d_total,
+                                        uint64_t *d_queue, void *stream) {
+  GARY_CHECK_ARG(variant >= GARY_ISECT_AUTO && variant <= GARY_ISECT_BITMAP, "unknown variant %d",
+                 variant);
+  GARY_CHECK_ARG(npairs == 0 || (d_a_off && d_a_len && d_a && d_b_off && d_b_len && d_b),
+                 "NULL list argument");
+  GARY_CHECK_ARG(!d_ex_off || d_ex, "d_ex is NULL while d_ex_off is set");
+  GARY_CHECK_ARG(d_queue != nullptr, "d_queue (one device word of scheduler state) is NULL");
+  cudaStream_t s = as_stream(stream);
+  GARY_CUDA(cudaMemsetAsync(d_queue, 0, 8, s));
+  if (d_total) GARY_CUDA(cudaMemsetAsync(d_total, 0, 8, s));
+  if (!npairs) return GARY_OK;
+  int per_sm = 0;
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_intersect_pairs, kSoWarps * 32, 0));
+  if (per_sm < 1) per_sm = 1;
+  const PairView pv{d_a_off, d_b_off, d_a_len, d_b_len, d_a, d_b};
+  const PairOut po{d_counts, nullptr, nullptr};
+  k_intersect_pairs<<<(unsigned)(sm_count() * per_sm), kSoWarps * 32, 0, s>>>(
+      pv, npairs, variant, po, PairFilter{d_bound, d_ex_off, d_ex},
+      reinterpret_cast<unsigned long long *>(d_queue), reinterpret_cast<unsigned long long *>(d_total));
   GARY_CUDA(cudaGetLastError());
   return GARY_OK;
 }

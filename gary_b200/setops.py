@@ -130,6 +130,27 @@ def intersect(batch: PairBatch, variant: int = GARY_ISECT_AUTO, materialise: boo
     return counts, total
 
 
+def intersect_num(batch: PairBatch, bound=None, ex_off=None, ex=None, variant: int = GARY_ISECT_AUTO,
+                  stream=None):
+    """Per-pair |{x in A & B : x < bound[i], x not excluded}| (int64 tensor)
+    and total: the bounded / ancestor-filtered counts of pattern matching.
+    bound: per-pair uint32 tensor or None; ex_off (npairs + 1, int64) / ex
+    (uint32 ids): per-pair excluded ids, or None."""
+    import torch
+
+    dev = "cuda"
+    counts = torch.empty(batch.npairs, dtype=torch.int64, device=dev)
+    total = torch.zeros(1, dtype=torch.int64, device=dev)
+    queue = torch.zeros(1, dtype=torch.int64, device=dev)
+    check(load().gary_intersect_num_batch(
+        batch.npairs, batch.a_off.data_ptr(), batch.la.data_ptr(), batch.a.data_ptr(),
+        batch.b_off.data_ptr(), batch.lb.data_ptr(), batch.b.data_ptr(), variant,
+        bound.data_ptr() if bound is not None else None, ex_off.data_ptr() if ex_off is not None else None,
+        ex.data_ptr() if ex is not None else None, counts.data_ptr(), total.data_ptr(), queue.data_ptr(),
+        _s(stream)), "gary_intersect_num_batch")
+    return counts, total
+
+
 def search(lst, keys, cache_entries: int = 0, stream=None):
     """(found uint8 tensor, count) for keys in the sorted list (device tensors)."""
     import torch

@@ -141,3 +141,47 @@ template <typename T = vidT>
 CUDA_INLINE DEVICE_ONLY T intersect(T *a, T size_a, T *b, T size_b, T *c) {
   return intersect_bs_cache(a, size_a, b, size_b, c);
 }
+
+// ---- bounded / ancestor-filtered counts -----------------------------------
+// The intersect_num family the reference leaves commented out
+// (Intersection.cuh:361-485), for pattern matching with symmetry breaking:
+// the lane's share of |{x in a & b : x < upper_bound, x not an ancestor}|.
+// Both lists are cut at the bound first (the reference stops its loop at the
+// first key past the bound), then the shorter one is searched in the longer.
+namespace gary_detail {
+template <typename T, typename Keep>
+CUDA_INLINE DEVICE_ONLY T count_bounded(T *a, T size_a, T *b, T size_b, T upper_bound, Keep keep) {
+  Span<T, void> sa(a, (size_t)size_a), sb(b, (size_t)size_b);
+  sa = Span<T, void>(a, gary_lower_bound(sa, sa.size(), upper_bound));
+  sb = Span<T, void>(b, gary_lower_bound(sb, sb.size(), upper_bound));
+  if (sa.size() == 0 || sb.size() == 0) return 0;
+  order_by_size(sa, sb);
+  return (T)probe_all(sa, [&](std::remove_cv_t<T> k) { return keep(k) && binary_search(sb, k); },
+                      (std::remove_cv_t<T> *)nullptr);
+}
+}  // namespace gary_detail
+
+template <typename T = vidT>
+CUDA_INLINE DEVICE_ONLY T intersect_num(T *a, T size_a, T *b, T size_b) {
+  return gary_detail::count_bounded(a, size_a, b, size_b, (T)~(T)0, [](T) { return true; });
+}
+
+template <typename T = vidT>
+CUDA_INLINE DEVICE_ONLY T intersect_num(T *a, T size_a, T *b, T size_b, T upper_bound) {
+  return gary_detail::count_bounded(a, size_a, b, size_b, upper_bound, [](T) { return true; });
+}
+
+template <typename T = vidT>
+CUDA_INLINE DEVICE_ONLY T intersect_num(T *a, T size_a, T *b, T size_b, T upper_bound, T ancestor) {
+  return gary_detail::count_bounded(a, size_a, b, size_b, upper_bound,
+                                    [&](T k) { return k != ancestor; });
+}
+
+template <typename T = vidT>
+CUDA_INLINE DEVICE_ONLY T intersect_num(T *a, T size_a, T *b, T size_b, T *ancestor, int n) {
+  return gary_detail::count_bounded(a, size_a, b, size_b, (T)~(T)0, [&](T k) {
+    for (int j = 0; j < n; ++j)
+      if (k == ancestor[j]) return false;
+    return true;
+  });
+}

@@ -243,6 +243,19 @@ int gary_intersect_batch(uint64_t npairs, const uint64_t *d_a_off, const uint32_
                          const uint64_t *d_out_off, uint32_t *d_out, uint64_t *d_total,
                          uint64_t *d_queue, void *stream);
 
+/* Bounded and ancestor-filtered counts: the reference's intersect_num family
+ * (include/ops/Intersection.cuh:361-485, left commented out there), used by
+ * pattern matching with symmetry breaking.  d_counts[i] = the number of x in
+ * A_i & B_i with x < d_bound[i] (d_bound NULL: no bound) and x not among the
+ * excluded ids d_ex[d_ex_off[i] .. d_ex_off[i+1]) (d_ex_off NULL: none; an id
+ * listed twice is excluded once).  Count only; arguments otherwise as
+ * gary_intersect_batch. */
+int gary_intersect_num_batch(uint64_t npairs, const uint64_t *d_a_off, const uint32_t *d_a_len,
+                             const uint32_t *d_a, const uint64_t *d_b_off, const uint32_t *d_b_len,
+                             const uint32_t *d_b, int variant, const uint32_t *d_bound,
+                             const uint64_t *d_ex_off, const uint32_t *d_ex, uint64_t *d_counts,
+                             uint64_t *d_total, uint64_t *d_queue, void *stream);
+
 /* Search nkeys keys in one sorted list (duplicates allowed).  cache_entries = 0:
  * binary_search (include/ops/Search.cuh:48-61); otherwise the two-phase search
  * of Search.cuh:93-138 with that many samples cached per CTA (the reference

@@ -71,6 +71,20 @@ __global__ void k_pairs(const uint32_t *a, const uint64_t *aoff, const uint32_t 
   }
 }
 
+// intersect_num with an upper bound and one ancestor, per pair (warp per pair)
+__global__ void k_pairs_num(const uint32_t *a, const uint64_t *aoff, const uint32_t *alen,
+                            const uint32_t *b, const uint64_t *boff, const uint32_t *blen,
+                            const uint32_t *bound, const uint32_t *anc, uint32_t npairs,
+                            uint32_t *counts) {
+  const uint32_t warp = threadIdx.x / WARP_SIZE, warps = blockDim.x / WARP_SIZE;
+  for (uint32_t p = blockIdx.x * warps + warp; p < npairs; p += gridDim.x * warps) {
+    uint32_t *A = const_cast<uint32_t *>(a + aoff[p]), *B = const_cast<uint32_t *>(b + boff[p]);
+    const uint32_t mine = intersect_num(A, alen[p], B, blen[p], bound[p], anc[p]);
+    const unsigned long long tot = graph_query::detail::warp_total((unsigned long long)mine);
+    if ((threadIdx.x & 31) == 0) counts[p] = (uint32_t)tot;
+  }
+}
+
 // the warp-level two-phase search (Search.cuh:140-170 form): lane l searches keys[l + 32 k]
 __global__ void k_search(const uint32_t *list, uint32_t n, const uint32_t *keys, uint32_t nkeys,
                          uint8_t *found) {
@@ -246,6 +260,29 @@ int main(int argc, char **argv) {
       for (size_t k = 0; ok && k < e.size(); ++k) ok = out[ooff[p] + k] == e[k];
       pair_bad += !ok;
     }
+  }
+
+  // ---- bounded, ancestor-filtered counts against the host
+  {
+    std::vector<uint32_t> bound(npairs), anc(npairs), want(npairs);
+    for (uint32_t p = 0; p < npairs; ++p) {
+      bound[p] = (uint32_t)(rng() % 20001);
+      const auto &e = expect[p];
+      anc[p] = e.empty() ? 0u : e[rng() % e.size()];
+      uint32_t c = 0;
+      for (uint32_t x : e) c += x < bound[p] && x != anc[p];
+      want[p] = c;
+    }
+    uint32_t *dbd, *dan;
+    CK(cudaMalloc(&dbd, npairs * 4));
+    CK(cudaMalloc(&dan, npairs * 4));
+    CK(cudaMemcpy(dbd, bound.data(), npairs * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dan, anc.data(), npairs * 4, cudaMemcpyHostToDevice));
+    k_pairs_num<<<148, 256>>>(dA, dao, dal, dB, dbo, dbl, dbd, dan, npairs, dcnt);
+    CK(cudaGetLastError());
+    std::vector<uint32_t> got(npairs);
+    CK(cudaMemcpy(got.data(), dcnt, npairs * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t p = 0; p < npairs; ++p) pair_bad += got[p] != want[p];
   }
 
   // ---- warp-level two-phase search against std::binary_search

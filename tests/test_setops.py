@@ -153,3 +153,47 @@ def test_search_large(cuda):
     for cache in (0, 32, 4096):
         found, count = so.search(dl, dk, cache)
         assert np.array_equal(found.cpu().numpy(), want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", ["auto", "merge", "search", "bitmap"])
+def test_intersect_num_bounded_and_filtered(cdf, cuda, variant):
+    """The intersect_num family: members below a per-pair bound and outside a
+    per-pair list of excluded ids (with repeats), against the oracle's merge."""
+    import torch
+
+    npairs = 2000
+    batch = so.PairBatch.generate(9, 300, npairs, cdf, 0.5)
+    rng = np.random.default_rng(3)
+    bound = rng.integers(0, 1 << 26, npairs).astype(np.uint32)
+    bound[::7] = 0xFFFFFFFF  # no effective bound
+    bound[::11] = 0          # empty range
+    pairs = [so.gen_pair_host(9, 300 + i, cdf, 0.5) for i in range(npairs)]
+    ex, ex_off = [], [0]
+    for a, b in pairs:
+        common = O.intersect(a, b, materialise=True)
+        k = int(rng.integers(0, 5))
+        pick = list(rng.choice(common, size=min(k, len(common)), replace=False)) if len(common) else []
+        pick += [int(rng.integers(0, 1 << 26))]          # usually not a member
+        if pick:
+            pick.append(pick[0])                          # a repeat is excluded once
+        ex += pick
+        ex_off.append(len(ex))
+    dev = lambda x, dt: torch.from_numpy(np.asarray(x, dt).view(dt)).cuda()  # noqa: E731
+    tb = dev(bound.view(np.int32), np.int32)
+    teo = dev(ex_off, np.int64)
+    tex = dev(np.asarray(ex, np.uint32).view(np.int32), np.int32)
+    counts, total = so.intersect_num(batch, tb, teo, tex, so.VARIANTS[variant])
+    counts = counts.cpu().numpy()
+    want_total = 0
+    for i, (a, b) in enumerate(pairs):
+        common = O.intersect(a, b, materialise=True)
+        excl = set(ex[ex_off[i]:ex_off[i + 1]])
+        want = sum(1 for x in common if x < bound[i] and int(x) not in excl)
+        assert counts[i] == want, (variant, i)
+        want_total += want
+    assert int(total.item()) == want_total
+    # no bound and no exclusions: the plain counts
+    c0, t0 = so.intersect_num(batch, variant=so.VARIANTS[variant])
+    c1, t1 = so.intersect(batch, so.VARIANTS[variant])
+    assert torch.equal(c0, c1) and int(t0.item()) == int(t1.item())
