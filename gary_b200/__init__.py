@@ -294,3 +294,35 @@ def write_bin_csr(path, ptr, idx) -> None:
 
 
 __all__ += ["bin_info", "read_bin_csr", "read_bin_coo", "write_bin_csr", "GARY_BIN_CSR", "GARY_BIN_COO"]
+
+
+# ---- byte planes ------------------------------------------------------------
+def planes_split(words, plane_bytes: int, stream=None) -> list:
+    """Split a CUDA tensor of 4- or 8-byte words (int32/uint32/int64) into
+    word_bytes / plane_bytes CUDA tensors of plane_bytes-wide entries (plane j
+    = byte group j of every word, least significant first)."""
+    import torch
+
+    wb = words.element_size()
+    k = wb // plane_bytes
+    dt = {1: torch.uint8, 2: torch.int16, 4: torch.int32}[plane_bytes]
+    planes = [torch.empty(words.numel(), dtype=dt, device=words.device) for _ in range(k)]
+    arr = (C.c_void_p * k)(*[p.data_ptr() for p in planes])
+    check(load().gary_planes_split(words.data_ptr(), words.numel(), wb, plane_bytes, arr, _stream(stream)),
+          "gary_planes_split")
+    return planes
+
+
+def planes_join(planes: list, word_bytes: int, stream=None):
+    """Inverse of planes_split: a CUDA tensor of word_bytes-wide words."""
+    import torch
+
+    n = planes[0].numel()
+    pb = planes[0].element_size()
+    words = torch.empty(n, dtype=torch.int32 if word_bytes == 4 else torch.int64, device=planes[0].device)
+    arr = (C.c_void_p * len(planes))(*[p.data_ptr() for p in planes])
+    check(load().gary_planes_join(arr, n, word_bytes, pb, words.data_ptr(), _stream(stream)), "gary_planes_join")
+    return words
+
+
+__all__ += ["planes_split", "planes_join"]

@@ -134,6 +134,8 @@ SIGNATURES = {
     "gary_csr_device_ptrs": (_INT, [_P, C.POINTER(_P), C.POINTER(_P)]),
     "gary_csr_download": (_INT, [_P, _P, _P]),
     "gary_csr_free": (_INT, [_P]),
+    "gary_planes_split": (_INT, [_P, _U64, _INT, _INT, _P, _P]),
+    "gary_planes_join": (_INT, [_P, _U64, _INT, _INT, _P, _P]),
     "gary_bin_info": (_INT, [C.c_char_p, _P, _P, _P]),
     "gary_bin_read_csr": (_INT, [C.c_char_p, _P, _P]),
     "gary_bin_read_coo": (_INT, [C.c_char_p, _P, _P]),

@@ -329,6 +329,20 @@ int gary_csr_device_ptrs(const gary_csr *c, const uint64_t **ptr, const uint32_t
 int gary_csr_download(const gary_csr *c, uint64_t *ptr, uint32_t *idx);
 int gary_csr_free(gary_csr *c);
 
+/* ---- byte planes -------------------------------------------------------- *
+ * Split n words of word_bytes (4 or 8) into word_bytes / plane_bytes planes
+ * of plane_bytes (1, 2 or 4, smaller than the word): plane j holds bytes
+ * [j * plane_bytes, (j+1) * plane_bytes) of every word, least significant
+ * first, in word order.  Replaces the reference's segmentKernel<SrcT, DstT>
+ * (include/kernels/SegmentArray.cuh:26-149; its tests, test/CUDATest.cu:60-130).
+ * gary_planes_join is the inverse.  d_planes is a HOST array of
+ * word_bytes / plane_bytes device pointers; every device pointer must be
+ * 16-byte aligned (GARY_ERR_INVALID otherwise).  Asynchronous on `stream`. */
+int gary_planes_split(const void *d_words, uint64_t n, int word_bytes, int plane_bytes,
+                      void *const *d_planes, void *stream);
+int gary_planes_join(void *const *d_planes, uint64_t n, int word_bytes, int plane_bytes, void *d_words,
+                     void *stream);
+
 /* ---- the reference's graph binaries (host only, no device use) -------- *
  * Read and write the files the reference saves with cereal's binary archive
  * (GraphCSR / GraphCOO save/load, include/Graph.h:132-148, 269-285; the
