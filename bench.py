@@ -57,9 +57,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU sample time")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference GPU kernel")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--workload", choices=["tc", "setops", "batch"], default="tc",
+    ap.add_argument("--workload", choices=["tc", "setops", "batch", "patterns"], default="tc",
                     help="tc: the headline triangle count; setops: the set-intersection microbench; "
-                         "batch: 4096 graphs in one launch")
+                         "batch: 4096 graphs in one launch; patterns: triangle / 4-cycle / 4-clique "
+                         "counts on the RMAT graph")
+    ap.add_argument("--patterns", default="3,4,5",
+                    help="patterns workload: 3 triangle, 4 four-cycle, 5 four-clique")
     ap.add_argument("--graphs", type=int, default=4096, help="batch: number of graphs")
     ap.add_argument("--no-autotune", action="store_true", help="batch: keep the default tile shapes")
     ap.add_argument("--pairs-log2", type=int, default=24, help="setops: total pairs = 2^k")
@@ -625,6 +628,47 @@ def run_batch(args, dist):
     return 0
 
 
+def run_patterns(args, dist):
+    """Triangle, 4-cycle and 4-clique counts of the seeded RMAT graph (one GPU):
+    per pattern the first call (plan building included, wall clock) and the
+    mean of `steps` counts after `warmup` (CUDA events on the counting stream,
+    plan cached).  One JSON line per pattern."""
+    import torch
+
+    import gary_b200 as gb
+    from gary_b200 import _lib
+
+    torch.cuda.set_device(dist.local)
+    n, csr = build_graph(gb, torch, args.scale, args.ef, args.seed)
+    g = upload_from_device_csr(gb, csr, n)
+    csr.free()
+    stream = torch.cuda.Stream()
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    names = {3: "triangle", 4: "4-cycle", 5: "4-clique"}
+    for pat in (int(x) for x in args.patterns.split(",")):
+        with torch.cuda.stream(stream):
+            t0 = time.perf_counter()
+            g.count_async(out, pat, stream=stream)
+            stream.synchronize()
+            first_s = time.perf_counter() - t0
+            for _ in range(args.warmup):
+                g.count_async(out, pat, stream=stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                g.count_async(out, pat, stream=stream)
+            e1.record(stream)
+        stream.synchronize()
+        ms = e0.elapsed_time(e1) / max(args.steps, 1)
+        print(json.dumps({"metric": f"{names[pat]} count time", "value": ms, "unit": "ms", "higher_is_better": False,
+                          "pattern": names[pat], "count": int(out.item()), "first_call_s": first_s,
+                          "steps": args.steps, "warmup": args.warmup, "n_gpus": 1, "data": "synthetic",
+                          "config": {"workload": f"{names[pat]} count, RMAT scale {args.scale} edge factor "
+                                                 f"{args.ef}, seed {args.seed}"}}), flush=True)
+    g.free()
+    return 0
+
+
 def load_lib():
     from gary_b200 import _lib
     return _lib.load()
@@ -639,6 +683,8 @@ def main():
         return run_setops(args, dist)
     if args.workload == "batch":
         return run_batch(args, dist)
+    if args.workload == "patterns":
+        return run_patterns(args, dist)
     if args.impl == "reference":
         return run_reference(args, dist)
     return run_ours(args, dist)

@@ -3,7 +3,7 @@
 
     python -m gary_b200.costmodel train --scales 18,19,20,21,22 \
         --out gary_b200/data/cost_model.gmlp
-    python -m gary_b200.costmodel eval --model gary_b200/data/cost_model.gmlp --scale 24
+    python -m gary_b200.costmodel eval --model gary_b200/data/cost_model.gmlp --scale 24 [--bound]
 
 Training data is logged by the instrumented plain kernel itself: for every
 middle vertex of the triangle kernel, clock64 cycles with each intersection
@@ -195,6 +195,27 @@ def time_scheds(g, steps: int = 5):
     return res
 
 
+def variant_bound(g, model: "CostModel | None" = None) -> dict:
+    """What per-vertex variant choice can gain on graph g: every warp-class
+    middle vertex is run with each legal variant forced; returns the summed
+    cycles of the plain dispatch, of the best legal variant per vertex (the
+    bound), and (with a model) of the model's choices."""
+    x, legal, cyc, cnt = profile(g, variants=(-1, 0, 1, 2, 3))
+    w = legal != 0
+    C_ = np.stack([cyc[k][w] for k in range(N_OUT)], 1)
+    ok = np.stack([((legal[w] >> k) & 1).astype(bool) & (cyc[k][w] > 0) for k in range(N_OUT)], 1)
+    best = np.where(ok, C_, np.inf).min(1)
+    best = np.where(np.isfinite(best), best, cyc[-1][w])
+    res = {"warp_vertices": int(w.sum()), "plain_cycles": float(cyc[-1][w].sum()),
+           "best_cycles": float(best.sum()), "bound_gain": float(cyc[-1][w].sum() / best.sum()),
+           "count": cnt}
+    if model is not None and w.any():
+        pred = model.predict(x[w])
+        choice = np.where(ok, pred, np.inf).argmin(1)
+        res["model_cycles"] = float(C_[np.arange(len(C_)), choice].sum())
+    return res
+
+
 def _graph(scale: int, ef: int, seed: int):
     import torch
 
@@ -229,6 +250,8 @@ def main(argv=None):
     e.add_argument("--model", default=str(DEFAULT_MODEL))
     e.add_argument("--scale", type=int, default=24)
     e.add_argument("--ef", type=int, default=32)
+    e.add_argument("--bound", action="store_true",
+                   help="also profile every variant per vertex and report the per-vertex choice bound")
     a = ap.parse_args(argv)
     if a.cmd == "train":
         Xs, Ts, Ms = [], [], []
@@ -252,7 +275,10 @@ def main(argv=None):
         model = CostModel.load(a.model)
         model.install()
         g = _graph(a.scale, a.ef, 1)
-        print(json.dumps({"scale": a.scale, "ef": a.ef, **time_scheds(g)}), flush=True)
+        res = {"scale": a.scale, "ef": a.ef, **time_scheds(g)}
+        if a.bound:
+            res["variant_choice"] = variant_bound(g, model)
+        print(json.dumps(res), flush=True)
         g.free()
 
 
