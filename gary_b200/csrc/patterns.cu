@@ -12,8 +12,9 @@
 // and looking every id up in a shared id -> position hash of N+(u).  Then
 //   K4(u) = sum over set bits (i, j) of popcount(row_i AND row_j),
 // since row j holds only positions after j.  Vertices with d <= 128 run on
-// one warp (rows of at most 4 words); larger ones take a whole CTA, with
-// rows in shared memory up to d = 1024 and in a per-CTA HBM buffer beyond.
+// one warp (rows of at most 4 words), d <= 512 on a 256-thread CTA, larger
+// ones on a 1024-thread CTA, with rows in shared memory up to d = 1024 and in
+// a per-CTA HBM buffer beyond.
 //
 // 4-cycles (symmetric ranked lists): each cycle is counted once at its
 // highest-ranked vertex u, with w the opposite vertex:
@@ -258,7 +259,7 @@ __device__ __forceinline__ void walk_ranges(const uint32_t *__restrict__ adj, ui
 
 // Tile {v0 = u, v1 = pre, j0 = wa, j1 = wb}: windows [wa, wb) of vertex u,
 // i.e. wedge ends w in [wa * kWinWords, min(wb * kWinWords, u)).
-__global__ void __launch_bounds__(kWinThreads, 1)
+__global__ void __launch_bounds__(kWinThreads)
     k_c4_win(GraphView s, const Tile *__restrict__ tiles, uint32_t t_lo, uint32_t t_hi,
              uint32_t *__restrict__ cursors, uint32_t max_pre, SchedState *sched,
              unsigned long long *__restrict__ out) {
@@ -360,17 +361,24 @@ __global__ void __launch_bounds__(kWinThreads, 1)
 }
 
 // ---- K4: bit rows of the subgraph induced by N+(u) -------------------------
-constexpr int kK4Threads = 1024;
-constexpr int kK4Warps = kK4Threads / 32;
-constexpr uint32_t kK4SmemWords = 49152;      // 192 KiB
-constexpr uint32_t kK4CtaLog = 13;            // CTA position hash: 8192 slots (d <= 4096)
-constexpr uint32_t kK4CtaRowWords = 32768;    // rows in shared memory when d * W fits
+// Three sizes of worker, so that no worker waits at barriers it does not need:
+//   warp vertices (3 <= d+ <= 128): one warp each, 8-warp CTAs, several per SM;
+//   mid vertices (128 < d+ <= 512): a 256-thread CTA each, rows in 32 KiB of
+//     shared memory, several CTAs per SM (one waits at a barrier, others run);
+//   big vertices (d+ > 512): a 1024-thread CTA each, rows in shared memory up
+//     to d+ = 1024 and in a per-CTA HBM buffer beyond.
 constexpr uint32_t kK4WarpMaxD = 128;         // warp vertices: rows of at most 4 words
-constexpr uint32_t kK4WarpLog = 8;            // warp position hash: 256 slots
-constexpr uint32_t kK4WarpWords = kK4SmemWords / kK4Warps;  // 1536 words per warp
+constexpr uint32_t kK4MidMaxD = 512;          // mid vertices: rows of at most 16 words
+constexpr int kK4WarpLog = 8;                 // warp position hash: 256 slots
+constexpr uint32_t kK4WarpWords = 1536;       // shared words per warp
+constexpr int kK4WarpCtaWarps = 8;
+constexpr int kK4MidThreads = 256, kK4MidLog = 10;
+constexpr uint32_t kK4MidRowWords = kK4MidMaxD * (kK4MidMaxD / 32);  // 8192
+constexpr int kK4BigThreads = 1024, kK4BigLog = 13;                 // d+ <= 4096
+constexpr uint32_t kK4BigRowWords = 32768;
 static_assert(2 * (1u << kK4WarpLog) + kK4WarpMaxD * (kK4WarpMaxD / 32) <= kK4WarpWords,
               "warp region too small");
-static_assert(2 * (1u << kK4CtaLog) + kK4CtaRowWords <= kK4SmemWords, "CTA region too small");
+static_assert((1u << kK4MidLog) >= 2 * kK4MidMaxD, "mid hash too small");
 
 __device__ __forceinline__ void pos_insert(uint32_t *keys, uint32_t *pos, uint32_t mask, int shift,
                                            uint32_t x, uint32_t p) {
@@ -463,48 +471,54 @@ __device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t
   return cnt;
 }
 
-__global__ void __launch_bounds__(kK4Threads, 1)
-    k_k4(GraphView g, const uint32_t *__restrict__ cta_list, uint32_t c_lo, uint32_t c_hi,
-         const uint32_t *__restrict__ warp_list, uint32_t w_lo, uint32_t w_hi,
-         uint32_t *__restrict__ pool, uint64_t pool_words, SchedState *sched,
-         unsigned long long *__restrict__ out) {
+// One listed vertex per CTA at a time, claimed through *counter.
+template <int THREADS, int HLOG, uint32_t ROWW>
+__global__ void __launch_bounds__(THREADS)
+    k_k4_cta(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
+             uint32_t *__restrict__ pool, uint64_t pool_words, uint32_t *counter,
+             unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t sm[];
   __shared__ uint32_t s_idx;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *keys = sm, *pos = sm + (1u << HLOG), *srows = sm + 2 * (1u << HLOG);
+  for (uint32_t i = threadIdx.x; i < (1u << HLOG); i += blockDim.x) keys[i] = kSentinel;
+  for (uint32_t i = threadIdx.x; i < ROWW; i += blockDim.x) srows[i] = 0;
   unsigned long long cnt = 0;
-  // phase 1: CTA vertices, largest first
-  {
-    uint32_t *keys = sm, *pos = sm + (1u << kK4CtaLog), *srows = sm + 2 * (1u << kK4CtaLog);
-    for (uint32_t i = threadIdx.x; i < (1u << kK4CtaLog); i += blockDim.x) keys[i] = kSentinel;
-    for (uint32_t i = threadIdx.x; i < kK4CtaRowWords; i += blockDim.x) srows[i] = 0;
-    while (true) {
-      if (threadIdx.x == 0) s_idx = c_lo + atomicAdd(&sched->next_cta, 1u);
-      __syncthreads();
-      const uint32_t k = s_idx;
-      __syncthreads();  // every thread has read s_idx
-      if (k >= c_hi) break;
-      const uint32_t u = cta_list[k];
-      const uint32_t d = g.row[u].y;
-      const uint64_t words = (uint64_t)d * ((d + 31) >> 5);
-      uint32_t *rows = words <= kK4CtaRowWords ? srows : pool + (uint64_t)blockIdx.x * pool_words;
-      cnt += k4_vertex(g, u, keys, pos, kK4CtaLog, rows, threadIdx.x, blockDim.x,
-                       [] { __syncthreads(); });
-    }
+  while (true) {
+    if (threadIdx.x == 0) s_idx = lo + atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t k = s_idx;
+    __syncthreads();  // every thread has read s_idx
+    if (k >= hi) break;
+    const uint32_t u = list[k];
+    const uint32_t d = g.row[u].y;
+    const uint64_t words = (uint64_t)d * ((d + 31) >> 5);
+    uint32_t *rows = words <= ROWW ? srows : pool + (uint64_t)blockIdx.x * pool_words;
+    cnt += k4_vertex(g, u, keys, pos, HLOG, rows, threadIdx.x, blockDim.x, [] { __syncthreads(); });
   }
-  // phase 2: warp vertices, each warp in its own region of shared memory
+  cnt = warp_sum_u64(cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
+// Warp vertices: each warp in its own region of shared memory, 32 vertices per claim.
+__global__ void __launch_bounds__(kK4WarpCtaWarps * 32)
+    k_k4_warp(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
+              uint32_t *counter, unsigned long long *__restrict__ out) {
+  extern __shared__ __align__(16) uint32_t sm[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *keys = sm + warp * kK4WarpWords, *pos = keys + (1u << kK4WarpLog),
            *rows = pos + (1u << kK4WarpLog);
   for (uint32_t i = lane; i < (1u << kK4WarpLog); i += 32) keys[i] = kSentinel;
   for (uint32_t i = lane; i < kK4WarpMaxD * (kK4WarpMaxD / 32); i += 32) rows[i] = 0;
   __syncwarp();
+  unsigned long long cnt = 0;
   while (true) {
     uint32_t c = 0;
-    if (lane == 0) c = atomicAdd(&sched->next_warp, 32u);
+    if (lane == 0) c = atomicAdd(counter, 32u);
     c = __shfl_sync(kFull, c, 0);
-    const uint32_t i0 = w_lo + c;
-    if (i0 >= w_hi) break;
-    const uint32_t nb = min(32u, w_hi - i0);
-    const uint32_t myu = lane < nb ? warp_list[i0 + lane] : 0u;
+    const uint32_t i0 = lo + c;
+    if (i0 >= hi) break;
+    const uint32_t nb = min(32u, hi - i0);
+    const uint32_t myu = lane < nb ? list[i0 + lane] : 0u;
     for (uint32_t q = 0; q < nb; ++q)
       cnt += k4_vertex(g, __shfl_sync(kFull, myu, q), keys, pos, kK4WarpLog, rows, lane, 32,
                        [] { __syncwarp(); });
@@ -631,12 +645,23 @@ struct MaxU32 {
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// The window kernel's shared-memory opt-in, once per device.
+int c4_win_attr() {
+  static bool done[64] = {false};
+  const int dev = device_ordinal();
+  if (dev < 64 && done[dev]) return GARY_OK;
+  GARY_CUDA(cudaFuncSetAttribute(k_c4_win, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kWinWords * 4)));
+  if (dev < 64) done[dev] = true;
+  return GARY_OK;
+}
+
 int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
   auto plan = std::make_unique<PatternPlan>();
   const uint32_t n = g->n;
   auto pol = thrust::cuda::par_nosync.on(s);
   const uint32_t *dp = g->dag.outdeg.p;
-  // warp vertices (3 <= d+ <= 128) in id order; CTA vertices largest first
+  // warp and mid vertices in id order; big vertices largest first
   GARY_TRY(plan->light.alloc_persistent(std::max<uint32_t>(n, 1)));
   plan->n_light = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
                                              thrust::counting_iterator<uint32_t>(n), plan->light.p,
@@ -644,19 +669,23 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
   GARY_TRY(plan->mid.alloc_persistent(std::max<uint32_t>(n, 1)));
   plan->n_mid = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
                                            thrust::counting_iterator<uint32_t>(n), plan->mid.p,
-                                           DegIn{dp, kK4WarpMaxD + 1, 0xFFFFFFFFu}) - plan->mid.p);
-  if (plan->n_mid) {
+                                           DegIn{dp, kK4WarpMaxD + 1, kK4MidMaxD}) - plan->mid.p);
+  GARY_TRY(plan->big.alloc_persistent(std::max<uint32_t>(n, 1)));
+  plan->n_big = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                           thrust::counting_iterator<uint32_t>(n), plan->big.p,
+                                           DegIn{dp, kK4MidMaxD + 1, 0xFFFFFFFFu}) - plan->big.p);
+  if (plan->n_big) {
     DevBuf<uint32_t> key;
-    GARY_TRY(key.alloc(plan->n_mid, s));
-    thrust::transform(pol, plan->mid.p, plan->mid.p + plan->n_mid, key.p, DegOf{dp});
-    thrust::sort_by_key(pol, key.p, key.p + plan->n_mid, plan->mid.p, thrust::greater<uint32_t>());
+    GARY_TRY(key.alloc(plan->n_big, s));
+    thrust::transform(pol, plan->big.p, plan->big.p + plan->n_big, key.p, DegOf{dp});
+    thrust::sort_by_key(pol, key.p, key.p + plan->n_big, plan->big.p, thrust::greater<uint32_t>());
     uint32_t dmax = 0;
     GARY_CUDA(cudaMemcpyAsync(&dmax, key.p, 4, cudaMemcpyDeviceToHost, s));
     GARY_CUDA(cudaStreamSynchronize(s));
     plan->max_pre = dmax;
     plan->win_ctas = (uint32_t)sm_count();
     const uint64_t words = (uint64_t)dmax * ((dmax + 31) / 32);
-    if (words > kK4CtaRowWords) {  // rows of the largest vertices live in HBM, one buffer per CTA
+    if (words > kK4BigRowWords) {  // rows of the largest vertices live in HBM, one buffer per CTA
       GARY_TRY(plan->cursors.alloc_persistent((uint64_t)plan->win_ctas * words));
       GARY_CUDA(cudaMemsetAsync(plan->cursors.p, 0, plan->cursors.bytes(), s));
     }
@@ -670,35 +699,56 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
 int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaStream_t s,
               uint32_t shard, uint32_t nshards) {
   auto part = [&](uint32_t total, uint32_t k) { return (uint32_t)((uint64_t)total * k / nshards); };
-  const uint32_t c0 = part(plan->n_mid, shard), c1 = part(plan->n_mid, shard + 1);
+  const uint32_t b0 = part(plan->n_big, shard), b1 = part(plan->n_big, shard + 1);
+  const uint32_t m0 = part(plan->n_mid, shard), m1 = part(plan->n_mid, shard + 1);
   const uint32_t w0 = part(plan->n_light, shard), w1 = part(plan->n_light, shard + 1);
-  const size_t smem = (size_t)kK4SmemWords * 4;
+  auto big = k_k4_cta<kK4BigThreads, kK4BigLog, kK4BigRowWords>;
+  auto mid = k_k4_cta<kK4MidThreads, kK4MidLog, kK4MidRowWords>;
+  const size_t smem_big = (2 * (1u << kK4BigLog) + kK4BigRowWords) * 4;
+  const size_t smem_mid = (2 * (1u << kK4MidLog) + kK4MidRowWords) * 4;
+  const size_t smem_warp = (size_t)kK4WarpCtaWarps * kK4WarpWords * 4;
   static bool attr[64] = {false};
   const int dev = device_ordinal();
   if (dev < 64 && !attr[dev]) {
-    GARY_CUDA(cudaFuncSetAttribute(k_k4, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GARY_CUDA(cudaFuncSetAttribute(big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_big));
+    GARY_CUDA(cudaFuncSetAttribute(mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mid));
+    GARY_CUDA(cudaFuncSetAttribute(k_k4_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_warp));
     attr[dev] = true;
   }
+  int per_mid = 0, per_warp = 0;
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_mid, mid, kK4MidThreads, smem_mid));
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_warp, k_k4_warp, kK4WarpCtaWarps * 32,
+                                                          smem_warp));
+  per_mid = std::max(per_mid, 1);
+  per_warp = std::max(per_warp, 1);
   const uint64_t dmax = plan->max_pre;
   const uint64_t pool_words = plan->cursors.p ? dmax * ((dmax + 31) / 32) : 0;
-  GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
+  SchedState *st = plan->sched.p;
+  GARY_CUDA(cudaMemsetAsync(st, 0, sizeof(SchedState), s));
   GARY_CUDA(cudaMemsetAsync(d_out, 0, 8, s));
   GARY_CUDA(cudaEventRecord(g->ev0, s));
-  if (c1 > c0 || w1 > w0) {
+  const GraphView gv = g->view();
+  if (b1 > b0) {
     // one CTA per SM; the pool holds one row buffer per CTA of the grid
-    const unsigned grid = (unsigned)sm_count();
+    const unsigned grid = std::min<unsigned>((unsigned)sm_count(), b1 - b0);
     if (plan->cursors.p && grid > plan->win_ctas) {
       set_error("4-clique row pool sized for %u CTAs, grid has %u", plan->win_ctas, grid);
       return GARY_ERR_INVALID;
     }
-    k_k4<<<grid, kK4Threads, smem, s>>>(g->view(), plan->mid.p, c0, c1, plan->light.p, w0, w1,
-                                        plan->cursors.p, pool_words, plan->sched.p, d_out);
+    big<<<grid, kK4BigThreads, smem_big, s>>>(gv, plan->big.p, b0, b1, plan->cursors.p, pool_words,
+                                              &st->next_cta, d_out);
   }
+  if (m1 > m0)
+    mid<<<std::min<unsigned>((unsigned)(sm_count() * per_mid), m1 - m0), kK4MidThreads, smem_mid, s>>>(
+        gv, plan->mid.p, m0, m1, nullptr, 0, &st->next_aux, d_out);
+  if (w1 > w0)
+    k_k4_warp<<<(unsigned)(sm_count() * per_warp), kK4WarpCtaWarps * 32, smem_warp, s>>>(
+        gv, plan->light.p, w0, w1, &st->next_warp, d_out);
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
-  g->last.tiles = (c1 - c0) + (w1 - w0);
-  g->last.cta_tiles = c1 - c0;
+  g->last.tiles = (b1 - b0) + (m1 - m0) + (w1 - w0);
+  g->last.cta_tiles = (b1 - b0) + (m1 - m0);
   g->last_timed = true;
   return GARY_OK;
 }
@@ -739,7 +789,13 @@ int build_c4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
   const uint32_t nh = (uint32_t)(thrust::copy_if(pol, big.p, big.p + nb, wed.p, heavy.p,
                                                  Above{kMidWedges}) - heavy.p);
   GARY_TRY(cost.alloc(std::max<uint32_t>(nh, 1), s));
-  plan->win_ctas = (uint32_t)sm_count();
+  GARY_TRY(c4_win_attr());
+  {
+    int per_sm = 0;
+    GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_win, kWinThreads,
+                                                            (size_t)kWinWords * 4));
+    plan->win_ctas = (uint32_t)(sm_count() * std::max(per_sm, 1));
+  }
   if (nh) {
     DevBuf<uint64_t> hw;
     GARY_TRY(hw.alloc(nh, s));
@@ -789,9 +845,9 @@ int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   if (dev < 64 && !attr[dev]) {
     GARY_CUDA(cudaFuncSetAttribute(k_c4_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_small));
     GARY_CUDA(cudaFuncSetAttribute(k_c4_mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mid));
-    GARY_CUDA(cudaFuncSetAttribute(k_c4_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_win));
     attr[dev] = true;
   }
+  GARY_TRY(c4_win_attr());
   int per_sm = 0;
   GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_small, kPWarps * 32, smem_small));
   if (per_sm < 1) per_sm = 1;
