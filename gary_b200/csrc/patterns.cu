@@ -259,21 +259,49 @@ __device__ __forceinline__ void walk_ranges(const uint32_t *__restrict__ adj, ui
 
 // Tile {v0 = u, v1 = pre, j0 = wa, j1 = wb}: windows [wa, wb) of vertex u,
 // i.e. wedge ends w in [wa * kWinWords, min(wb * kWinWords, u)).
+//
+// Per lower neighbour k (v = N(u)[k]) the CTA keeps, in its HBM scratch, v's
+// row record, a cursor into N(v), the cursor before the last window, and the
+// window index of the id at the cursor (nextw).  A window pass scans nextw,
+// compacts the neighbours whose next id falls in the window into an active
+// list, and only those gallop and walk; the pass also yields the next
+// non-empty window.  Neighbours with few ids below u are active in few
+// windows, so most passes touch a small part of the list.
+constexpr uint32_t kNoWindow = 0xFFFFFFFFu;
+
+struct C4Scratch {
+  uint2 *vrow;     // row record of each lower neighbour
+  uint32_t *cur, *prev, *nextw, *act;
+};
+
+__device__ __forceinline__ C4Scratch c4_scratch(uint32_t *base, uint32_t max_pre) {
+  C4Scratch c;
+  c.vrow = reinterpret_cast<uint2 *>(base);
+  c.cur = base + 2 * (uint64_t)max_pre;
+  c.prev = c.cur + max_pre;
+  c.nextw = c.prev + max_pre;
+  c.act = c.nextw + max_pre;
+  return c;
+}
+
+// words of scratch per lower neighbour (vrow 2, cur, prev, nextw, act)
+constexpr uint32_t kC4ScratchWords = 6;
+
 __global__ void __launch_bounds__(kWinThreads)
     k_c4_win(GraphView s, const Tile *__restrict__ tiles, uint32_t t_lo, uint32_t t_hi,
-             uint32_t *__restrict__ cursors, uint32_t max_pre, SchedState *sched,
+             uint32_t *__restrict__ scratch, uint32_t max_pre, SchedState *sched,
              unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t cnt[];  // kWinWords counters, zero between windows
-  __shared__ uint32_t s_tile, s_next, s_nextw;
+  __shared__ uint32_t s_tile, s_next, s_nact, s_minw;
   __shared__ unsigned long long s_wedges;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t *cur = cursors + (uint64_t)blockIdx.x * 2 * max_pre, *prev = cur + max_pre;
+  const C4Scratch cs = c4_scratch(scratch + (uint64_t)blockIdx.x * kC4ScratchWords * max_pre, max_pre);
   unsigned long long acc = 0;
   for (uint32_t i = threadIdx.x; i < kWinWords; i += blockDim.x) cnt[i] = 0;
   while (true) {
     if (threadIdx.x == 0) {
       s_tile = t_lo + atomicAdd(&sched->next_cta, 1u);
-      s_nextw = kSentinel;
+      s_minw = kNoWindow;
     }
     __syncthreads();
     const uint32_t t = s_tile;
@@ -284,49 +312,69 @@ __global__ void __launch_bounds__(kWinThreads)
     const uint64_t end64 = (uint64_t)tl.j1 * kWinWords, begin64 = (uint64_t)tl.j0 * kWinWords;
     const uint32_t w_end = end64 < u ? (uint32_t)end64 : u;
     const uint32_t w_begin = begin64 < w_end ? (uint32_t)begin64 : w_end;
-    // cursors at the tile's first window; the smallest id any of them sees
-    uint32_t first = kSentinel;
-    for (uint32_t i = threadIdx.x; i < pre; i += blockDim.x) {
-      const uint2 rv = s.row[au[i]];
+    // state at the tile's first window
+    uint32_t mw = kNoWindow;
+    for (uint32_t k = threadIdx.x; k < pre; k += blockDim.x) {
+      const uint2 rv = s.row[au[k]];
       const uint32_t *l = s.adj + (uint64_t)rv.x * 4;
       const uint32_t c = lower_bound_u32(l, 0, rv.y, w_begin);
-      cur[i] = c;
-      if (c < rv.y) first = min(first, l[c]);
+      const uint32_t x = c < rv.y ? l[c] : kSentinel;
+      const uint32_t nw = x < w_end ? x / kWinWords : kNoWindow;
+      cs.vrow[k] = rv;
+      cs.cur[k] = c;
+      cs.nextw[k] = nw;
+      mw = min(mw, nw);
     }
-    first = warp_min_u32(first);
-    if (lane == 0) atomicMin(&s_nextw, first);
+    mw = warp_min_u32(mw);
+    if (lane == 0) atomicMin(&s_minw, mw);
     __syncthreads();
     while (true) {
-      const uint32_t nw = s_nextw;
-      if (nw >= w_end) break;  // no id of the tile's range is left
-      const uint32_t lo = nw - nw % kWinWords;
+      const uint32_t win = s_minw;
+      if (win == kNoWindow) break;  // no id of the tile's range is left
+      const uint32_t lo = win * kWinWords;
       const uint32_t hi = lo + kWinWords < w_end ? lo + kWinWords : w_end;
-      __syncthreads();  // every thread has read s_nextw
+      __syncthreads();  // every thread has read s_minw
       if (threadIdx.x == 0) {
         s_next = 0;
-        s_nextw = kSentinel;
+        s_nact = 0;
+        s_minw = kNoWindow;
         s_wedges = 0;
       }
       __syncthreads();
-      // count: advance every cursor past the window, counting the ids passed
-      uint32_t nxt = kSentinel;
+      // active neighbours of this window; the others keep their next window
+      uint32_t mwi = kNoWindow;
+      for (uint32_t k = threadIdx.x; k < pre; k += blockDim.x) {
+        const uint32_t nw = cs.nextw[k];
+        if (nw == win) cs.act[atomicAdd(&s_nact, 1u)] = k;
+        else mwi = min(mwi, nw);
+      }
+      mwi = warp_min_u32(mwi);
+      if (lane == 0) atomicMin(&s_minw, mwi);
+      __syncthreads();
+      const uint32_t nact = s_nact;
+      // count: advance the active cursors past the window, counting the ids passed
+      uint32_t nxt = kNoWindow;
       unsigned long long seen = 0;
       while (true) {
         uint32_t k0 = 0;
         if (lane == 0) k0 = atomicAdd(&s_next, 32u);
         k0 = __shfl_sync(kFull, k0, 0);
-        if (k0 >= pre) break;
-        const uint32_t k = k0 + lane;
+        if (k0 >= nact) break;
+        const uint32_t a = k0 + lane;
         uint32_t q4 = 0, b = 0, e = 0;
-        if (k < pre) {
-          const uint2 rv = s.row[au[k]];
+        if (a < nact) {
+          const uint32_t k = cs.act[a];
+          const uint2 rv = cs.vrow[k];
           const uint32_t *l = s.adj + (uint64_t)rv.x * 4;
-          b = cur[k];
+          b = cs.cur[k];
           e = gallop_geq(l, b, rv.y, hi);
-          prev[k] = b;
-          cur[k] = e;
+          cs.prev[k] = b;
+          cs.cur[k] = e;
+          const uint32_t x = e < rv.y ? l[e] : kSentinel;
+          const uint32_t nw = x < w_end ? x / kWinWords : kNoWindow;
+          cs.nextw[k] = nw;
+          nxt = min(nxt, nw);
           q4 = rv.x;
-          if (e < rv.y) nxt = min(nxt, l[e]);
           seen += e - b;
         }
         walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { acc += atomicAdd(&cnt[w - lo], 1u); });
@@ -334,19 +382,20 @@ __global__ void __launch_bounds__(kWinThreads)
       nxt = warp_min_u32(nxt);
       seen = warp_sum_u64(seen);
       if (lane == 0) {
-        atomicMin(&s_nextw, nxt);
+        atomicMin(&s_minw, nxt);
         if (seen) atomicAdd(&s_wedges, seen);
       }
       __syncthreads();
       // zero the window again: walk the same ids when few, else clear it whole
-      if (s_wedges + pre < (hi - lo) / 4) {
-        for (uint32_t k0 = warp * 32; k0 < pre; k0 += kWinWarps * 32) {
-          const uint32_t k = k0 + lane;
+      if (s_wedges + nact < (hi - lo) / 4) {
+        for (uint32_t a0 = warp * 32; a0 < nact; a0 += kWinWarps * 32) {
+          const uint32_t a = a0 + lane;
           uint32_t q4 = 0, b = 0, e = 0;
-          if (k < pre) {
-            q4 = s.row[au[k]].x;
-            b = prev[k];
-            e = cur[k];
+          if (a < nact) {
+            const uint32_t k = cs.act[a];
+            q4 = cs.vrow[k].x;
+            b = cs.prev[k];
+            e = cs.cur[k];
           }
           walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { cnt[w - lo] = 0u; });
         }
@@ -822,7 +871,8 @@ int build_c4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
     k_c4_fill_tiles<<<grid_for(nh), kThreads, 0, s>>>(g->sym.row.p, g->dag.outdeg.p, heavy.p, nh, kt.p,
                                                       plan->tiles.p);
     GARY_CUDA(cudaGetLastError());
-    GARY_TRY(plan->cursors.alloc_persistent((uint64_t)plan->win_ctas * 2 * std::max(plan->max_pre, 1u)));
+    GARY_TRY(plan->cursors.alloc_persistent((uint64_t)plan->win_ctas * kC4ScratchWords *
+                                            std::max(plan->max_pre, 1u)));
   }
   GARY_TRY(plan->sched.alloc_persistent(1));
   GARY_CUDA(cudaStreamSynchronize(s));

@@ -17,7 +17,7 @@ struct PatternPlan {
   DevBuf<uint32_t> light;    // light vertices (K4 groups index it; C4 warps walk it)
   DevBuf<uint32_t> mid;      // C4: medium vertices, one CTA hash map each; K4: mid vertices
   DevBuf<uint32_t> big;      // K4: vertices with d+ > 512, largest first
-  DevBuf<uint32_t> cursors;  // C4: per window-kernel CTA, 2 x max_pre list positions
+  DevBuf<uint32_t> cursors;  // C4: per window-kernel CTA, 6 x max_pre words of list state; K4: row pool
   DevBuf<SchedState> sched;
   uint32_t n_cta = 0, n_warp = 0, n_light = 0, n_mid = 0, n_big = 0, max_pre = 0, win_ctas = 0;
 };
