@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--ef", type=int, default=32)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--sched", choices=["plain", "learned"], default="plain")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--e2e-input", choices=["dag", "symmetric"], default="dag",
                     help="host CSR the e2e leg uploads: the reference's id-oriented DAG or the symmetric graph")
     ap.add_argument("--pool-keep-gb", type=float, default=None,
@@ -339,12 +339,15 @@ def run_ours(args, dist):
             if k > 0:  # first one warms the allocator
                 e2e_times.append(dt)
             assert res.value == count_local, "e2e count differs from the resident-graph count"
-        e2e_s = dist.allreduce(sum(e2e_times) / len(e2e_times), "max")
+        # the median step: host-to-device copies share the host's PCIe links with
+        # other jobs, whose bursts show up as single slow steps (the mean is reported too)
+        e2e_s = dist.allreduce(statistics.median(e2e_times), "max")
+        e2e_mean = dist.allreduce(sum(e2e_times) / len(e2e_times), "max")
         form = ("id-oriented DAG CSR, rows list neighbours v < u (the reference's csr_dag input)"
                 if args.e2e_input == "dag" else "symmetric CSR")
         e2e = {"value": m / e2e_s, "unit": UNIT, "h2d_bytes_per_step": (n + 1) * 8 + e2e_nnz * 4,
-               "d2h_bytes_per_step": 8, "ms_per_step": e2e_s * 1e3,
-               "step_ms": [round(t * 1e3, 2) for t in e2e_times],
+               "d2h_bytes_per_step": 8, "ms_per_step": e2e_s * 1e3, "statistic": "median of the steps",
+               "mean_ms_per_step": e2e_mean * 1e3, "step_ms": [round(t * 1e3, 2) for t in e2e_times],
                "path": f"gary_graph_upload(pinned host {form}) + gary_count_shard_async + D2H of the count"}
     else:
         csr.free()
