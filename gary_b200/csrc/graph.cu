@@ -238,92 +238,227 @@ __global__ void k_rows_check_wedges(const uint2 *__restrict__ row, const uint32_
 }
 
 // ---- sorting the rows of a padded CSR in place ----------------------------
-// Rows of up to 32 ids: a warp ranks its lane values (ties by lane, so equal
-// ids stay adjacent and a duplicate check still sees them).  Rows of up to
-// kSortWarpMax ids: a warp bitonic-sorts them in its shared-memory slice.
-// Longer rows: a CTA bitonic sort up to kSortCtaMax ids; rarer longer ones
-// go to a library segmented sort.
+// Every row is sorted by a bitonic network held in registers:
+// - up to 32 ids: one id per lane, several rows per warp in aligned segments
+//   of 4, 8, 16 or 32 lanes (shuffles never leave a segment);
+// - up to kSortWarpMax ids: one warp, E = 2..32 ids per lane;
+// - up to kSortGroupMax ids: a group of 2, 4 or 8 warps with 32 ids per
+//   lane, exchanging through shared memory only for strides of 1024 and up;
+// - longer rows (rare): a library radix sort per row.
+// Rows start 32-byte aligned and are padded with kSentinel to plen, a multiple
+// of 8, so lanes load and store whole 8- or 16-byte vectors, positions from
+// plen on are sentinels without a load, and sentinels sort last.
 constexpr uint32_t kSortWarps = 8;
 constexpr uint32_t kSortWarpMax = 1024;
-constexpr uint32_t kSortCtaMax = 8192;
+constexpr uint32_t kSortGroupMax = 8192;
+constexpr int kSortGroupThreads = 256;
 
-template <typename Sync>
-__device__ __forceinline__ void bitonic_smem(uint32_t *a, uint32_t P, uint32_t tid, uint32_t nth, Sync sync) {
-  for (uint32_t k = 2; k <= P; k <<= 1) {
-    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-      for (uint32_t i = tid; i < P; i += nth) {
-        const uint32_t l = i ^ j;
-        if (l > i) {
-          const uint32_t x = a[i], y = a[l];
-          const bool up = (i & k) == 0;
-          if ((x > y) == up) {
-            a[i] = y;
-            a[l] = x;
-          }
-        }
-      }
-      sync();
+__device__ __forceinline__ uint32_t keep_side(bool keep_min, uint32_t a, uint32_t b) {
+  return keep_min ? min(a, b) : max(a, b);
+}
+
+// An S = 2^LOGS lane segment sorts one id per lane (sl = lane index in the segment).
+template <int LOGS>
+__device__ __forceinline__ uint32_t segment_sort(uint32_t x, int sl) {
+#pragma unroll
+  for (int lk = 1; lk <= LOGS; ++lk) {
+#pragma unroll
+    for (int lj = lk - 1; lj >= 0; --lj) {
+      const uint32_t y = __shfl_xor_sync(kFull, x, 1 << lj);
+      x = keep_side(((sl >> lj) & 1) == ((sl >> lk) & 1), x, y);
+    }
+  }
+  return x;
+}
+
+// The rows of a warp's chunk (records in lane j's rec) whose length lies in
+// (S/2, S] (from 2 for the smallest class): 32/S rows per pass, one segment each.
+template <int LOGS>
+__device__ __forceinline__ void sort_short_rows(uint2 rec, uint32_t *__restrict__ adj, int lane) {
+  constexpr int S = 1 << LOGS;
+  constexpr uint32_t lo = LOGS == 2 ? 2 : S / 2 + 1;
+  uint32_t mask = __ballot_sync(kFull, rec.y >= lo && rec.y <= (uint32_t)S);
+  const int seg = lane >> LOGS, sl = lane & (S - 1);
+  while (mask) {
+    const unsigned j = __fns(mask, 0, seg + 1);  // this segment's row, or none
+    const int src = j < 32 ? (int)j : 0;
+    const uint32_t rx = __shfl_sync(kFull, rec.x, src);
+    const uint32_t dj = __shfl_sync(kFull, rec.y, src);
+    const uint32_t d = j < 32 ? dj : 0u;
+    uint32_t *l = adj + (uint64_t)rx * 4;
+    uint32_t x = (uint32_t)sl < d ? l[sl] : kSentinel;
+    x = segment_sort<LOGS>(x, sl);
+    if ((uint32_t)sl < d) l[sl] = x;
+    const unsigned cut = __fns(mask, 0, 32 / S + 1);  // first row of the next pass
+    mask = cut < 32 ? mask & ~((1u << cut) - 1) : 0u;
+  }
+}
+
+// One warp's block of a bitonic network, E = 2^LOGE ids per lane: lane L
+// owns elements gbase .. gbase+E-1 of the row (gbase = its offset in the
+// row).  Strides below E compare two registers of one lane; strides below
+// 32E pair a register with the same register of lane L ^ (j/E).  The
+// direction of each comparison follows bit k of the element's index.
+template <int LOGE>
+__device__ __forceinline__ void warp_stage(uint32_t (&x)[1 << LOGE], int lane, uint32_t gbase, uint32_t k,
+                                           int lj) {
+  constexpr int E = 1 << LOGE;
+  if (lj >= LOGE) {
+    const int lm = 1 << (lj - LOGE);
+    const bool keep_min = ((lane & lm) == 0) == ((gbase & k) == 0);
+#pragma unroll
+    for (int e = 0; e < E; ++e) x[e] = keep_side(keep_min, x[e], __shfl_xor_sync(kFull, x[e], lm));
+  } else {
+    const uint32_t j = 1u << lj;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      if (e & j) continue;
+      const int f = e | j;
+      const bool up = k < (uint32_t)E ? (e & k) == 0 : (gbase & k) == 0;
+      const uint32_t lo = min(x[e], x[f]), hi = max(x[e], x[f]);
+      x[e] = up ? lo : hi;
+      x[f] = up ? hi : lo;
     }
   }
 }
 
+// All stages of the network whose sequence length k is at most 32E: sorts
+// the warp's block, ascending or descending by bit 32E of gbase.
+template <int LOGE>
+__device__ __forceinline__ void warp_sort_block(uint32_t (&x)[1 << LOGE], int lane, uint32_t gbase) {
+#pragma unroll
+  for (int lk = 1; lk <= LOGE + 5; ++lk)
+#pragma unroll
+    for (int lj = lk - 1; lj >= 0; --lj) warp_stage<LOGE>(x, lane, gbase, 1u << lk, lj);
+}
+
+// The strides below 32E of a merge of sequence length k > 32E.
+template <int LOGE>
+__device__ __forceinline__ void warp_merge_block(uint32_t (&x)[1 << LOGE], int lane, uint32_t gbase, uint32_t k) {
+#pragma unroll
+  for (int lj = LOGE + 4; lj >= 0; --lj) warp_stage<LOGE>(x, lane, gbase, k, lj);
+}
+
+// Sorts one padded row of up to 2^(LOGE+5+LOGW) ids with a group of 2^LOGW
+// warps (wg = warp index in the group): lane L of warp wg owns elements from
+// gbase = (wg*32 + L)*E.  Strides of 32E and up pair a register with the same
+// register of warp wg ^ (j/32E), through xs (layout [warp][e][lane]) and a
+// named barrier per group.
+template <int LOGE, int LOGW>
+__device__ __forceinline__ void group_sort_row(uint32_t *__restrict__ l, uint32_t plen, int lane, int wg,
+                                               uint32_t *xs, int bar_id) {
+  constexpr int E = 1 << LOGE;
+  constexpr int LOGWARP = LOGE + 5;
+  const uint32_t gbase = ((uint32_t)wg * 32 + lane) * E;
+  uint32_t x[E];
+  if constexpr (E == 2) {
+    uint2 v = make_uint2(kSentinel, kSentinel);
+    if (gbase < plen) v = *reinterpret_cast<const uint2 *>(l + gbase);
+    x[0] = v.x;
+    x[1] = v.y;
+  } else {
+#pragma unroll
+    for (int q = 0; q < E / 4; ++q) {
+      uint4 v = make_uint4(kSentinel, kSentinel, kSentinel, kSentinel);
+      if (gbase + 4 * q < plen) v = *reinterpret_cast<const uint4 *>(l + gbase + 4 * q);
+      x[4 * q] = v.x;
+      x[4 * q + 1] = v.y;
+      x[4 * q + 2] = v.z;
+      x[4 * q + 3] = v.w;
+    }
+  }
+  warp_sort_block<LOGE>(x, lane, gbase);
+  if constexpr (LOGW > 0) {
+#pragma unroll 1
+    for (int lk = LOGWARP + 1; lk <= LOGWARP + LOGW; ++lk) {
+      const uint32_t k = 1u << lk;
+#pragma unroll 1
+      for (int lj = lk - 1; lj >= LOGWARP; --lj) {
+        const int wm = 1 << (lj - LOGWARP);
+        const bool keep_min = ((wg & wm) == 0) == ((gbase & k) == 0);
+#pragma unroll
+        for (int e = 0; e < E; ++e) xs[(wg * E + e) * 32 + lane] = x[e];
+        asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(32 << LOGW) : "memory");
+#pragma unroll
+        for (int e = 0; e < E; ++e) x[e] = keep_side(keep_min, x[e], xs[((wg ^ wm) * E + e) * 32 + lane]);
+        asm volatile("bar.sync %0, %1;" ::"r"(bar_id), "r"(32 << LOGW) : "memory");
+      }
+      warp_merge_block<LOGE>(x, lane, gbase, k);
+    }
+  }
+  if constexpr (E == 2) {
+    if (gbase < plen) *reinterpret_cast<uint2 *>(l + gbase) = make_uint2(x[0], x[1]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < E / 4; ++q)
+      if (gbase + 4 * q < plen)
+        *reinterpret_cast<uint4 *>(l + gbase + 4 * q) = make_uint4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+  }
+}
+
+__device__ __forceinline__ uint32_t padded_len(uint32_t d) { return ((d + 7) >> 3) << 3; }
+
+// A warp takes 32 consecutive rows (one coalesced load of their records):
+// the short ones by segments, then the others up to kSortWarpMax one by one.
 __global__ void __launch_bounds__(kSortWarps * 32)
     k_sort_rows_warp(const uint2 *__restrict__ row, uint32_t n, uint32_t *__restrict__ adj) {
-  __shared__ uint32_t buf[kSortWarps * kSortWarpMax];
   const int lane = threadIdx.x & 31;
-  uint32_t *a = buf + (threadIdx.x >> 5) * kSortWarpMax;
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t u = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += warps) {
-    const uint2 r = row[u];
-    const uint32_t d = r.y;
-    if (d < 2 || d > kSortWarpMax) continue;
-    uint32_t *l = adj + (uint64_t)r.x * 4;
-    if (d <= 32) {
-      const uint32_t x = (uint32_t)lane < d ? l[lane] : kSentinel;
-      uint32_t rk = 0;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const uint32_t y = __shfl_sync(kFull, x, j);
-        rk += (y < x) || (y == x && j < lane);
-      }
-      __syncwarp();
-      if ((uint32_t)lane < d) l[rk] = x;
-      __syncwarp();
-      continue;
+  for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c * 32 < n; c += warps) {
+    const uint64_t u0 = c * 32;
+    const uint2 rec = u0 + lane < n ? row[u0 + lane] : make_uint2(0, 0);
+    sort_short_rows<2>(rec, adj, lane);
+    sort_short_rows<3>(rec, adj, lane);
+    sort_short_rows<4>(rec, adj, lane);
+    sort_short_rows<5>(rec, adj, lane);
+    uint32_t mask = __ballot_sync(kFull, rec.y > 32 && rec.y <= kSortWarpMax);
+    while (mask) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const uint32_t rx = __shfl_sync(kFull, rec.x, j), d = __shfl_sync(kFull, rec.y, j);
+      uint32_t *l = adj + (uint64_t)rx * 4;
+      const uint32_t plen = padded_len(d);
+      if (d <= 64) group_sort_row<1, 0>(l, plen, lane, 0, nullptr, 0);
+      else if (d <= 128) group_sort_row<2, 0>(l, plen, lane, 0, nullptr, 0);
+      else if (d <= 256) group_sort_row<3, 0>(l, plen, lane, 0, nullptr, 0);
+      else if (d <= 512) group_sort_row<4, 0>(l, plen, lane, 0, nullptr, 0);
+      else group_sort_row<5, 0>(l, plen, lane, 0, nullptr, 0);
     }
-    uint32_t P = 64;
-    while (P < d) P <<= 1;
-    for (uint32_t i = lane; i < P; i += 32) a[i] = i < d ? l[i] : kSentinel;
-    __syncwarp();
-    bitonic_smem(a, P, lane, 32, [] { __syncwarp(); });
-    for (uint32_t i = lane; i < d; i += 32) l[i] = a[i];
-    __syncwarp();
   }
 }
 
-__global__ void __launch_bounds__(512)
-    k_sort_rows_cta(const uint2 *__restrict__ row, const uint32_t *__restrict__ list, uint32_t nl,
-                    uint32_t *__restrict__ adj) {
-  __shared__ uint32_t a[kSortCtaMax];
-  for (uint32_t k = blockIdx.x; k < nl; k += gridDim.x) {
-    const uint2 r = row[list[k]];
-    const uint32_t d = r.y;
-    uint32_t *l = adj + (uint64_t)r.x * 4;
-    uint32_t P = 1024;
-    while (P < d) P <<= 1;
-    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) a[i] = i < d ? l[i] : kSentinel;
-    __syncthreads();
-    bitonic_smem(a, P, threadIdx.x, blockDim.x, [] { __syncthreads(); });
-    for (uint32_t i = threadIdx.x; i < d; i += blockDim.x) l[i] = a[i];
-    __syncthreads();
+// Rows longer than kSortWarpMax, sorted into lists by length class:
+// (1024, 2048], (2048, 4096], (4096, 8192] and longer.
+__global__ void k_long_rows(const uint2 *__restrict__ row, uint32_t n, uint32_t cap,
+                            uint32_t *__restrict__ lists, uint32_t *__restrict__ counts) {
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t d = row[u].y;
+    if (d <= kSortWarpMax) continue;
+    const int cls = d <= 2048 ? 0 : d <= 4096 ? 1 : d <= kSortGroupMax ? 2 : 3;
+    const uint32_t slot = atomicAdd(&counts[cls], 1u);
+    if (slot < cap) lists[(uint64_t)cls * cap + slot] = (uint32_t)u;
   }
 }
 
-struct RowLenIn {
-  const uint2 *row;
-  uint32_t lo, hi;
-  __host__ __device__ bool operator()(uint32_t u) const { return row[u].y > lo && row[u].y <= hi; }
-};
+// Rows of the length class of 2^LOGW warps per group; kSortGroupThreads /
+// (32 << LOGW) groups per CTA, each on its own rows and named barrier.
+template <int LOGW>
+__global__ void __launch_bounds__(kSortGroupThreads)
+    k_sort_rows_group(const uint2 *__restrict__ row, const uint32_t *__restrict__ list,
+                      const uint32_t *__restrict__ count, uint32_t cap, uint32_t *__restrict__ adj) {
+  constexpr int G = kSortGroupThreads / (32 << LOGW);
+  __shared__ uint32_t xs[kSortGroupThreads * 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = warp >> LOGW, wg = warp & ((1 << LOGW) - 1);
+  uint32_t *gx = xs + (uint32_t)g * (1024u << LOGW);
+  const uint32_t nl = min(*count, cap);
+  for (uint32_t t = blockIdx.x * G + g; t < nl; t += gridDim.x * G) {
+    const uint2 r = row[list[t]];
+    group_sort_row<5, LOGW>(adj + (uint64_t)r.x * 4, padded_len(r.y), lane, wg, gx, 1 + g);
+  }
+}
+
 struct RowOf {
   const uint2 *row;
   __host__ __device__ uint2 operator()(uint32_t u) const { return row[u]; }
@@ -585,26 +720,40 @@ int ranked_dag_by_rows(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz
   tr.mark("fill");
   // order every row in place
   if (m) {
-    k_sort_rows_warp<<<sm_count() * 8, kSortWarps * 32, 0, s>>>(c.row.p, n, c.adj.p);
+    int per_sm = 0;
+    GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sort_rows_warp, kSortWarps * 32, 0));
+    k_sort_rows_warp<<<sm_count() * std::max(per_sm, 1), kSortWarps * 32, 0, s>>>(c.row.p, n, c.adj.p);
     GARY_CUDA(cudaGetLastError());
-    DevBuf<uint32_t> big;
-    GARY_TRY(big.alloc(std::max<uint32_t>(n, 1), s));
-    const uint32_t nb = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
-                                                   thrust::counting_iterator<uint32_t>(n), big.p,
-                                                   RowLenIn{c.row.p, kSortWarpMax, kSortCtaMax}) - big.p);
-    if (nb) {
-      k_sort_rows_cta<<<std::min<uint32_t>(nb, sm_count() * 4), 512, 0, s>>>(c.row.p, big.p, nb, c.adj.p);
+    tr.mark("row sort: up to 1024 ids (warp)");
+    // at most m / 1025 rows are longer than 1024 ids
+    const uint32_t cap = (uint32_t)std::min<uint64_t>(n, m / (kSortWarpMax + 1) + 1);
+    DevBuf<uint32_t> lists, counts;
+    GARY_TRY(lists.alloc((uint64_t)cap * 4, s));
+    GARY_TRY(counts.alloc(4, s));
+    GARY_CUDA(cudaMemsetAsync(counts.p, 0, 16, s));
+    k_long_rows<<<grid_for(n), kThreads, 0, s>>>(c.row.p, n, cap, lists.p, counts.p);
+    GARY_CUDA(cudaGetLastError());
+    auto group_launch = [&](auto kern, int cls) -> int {
+      int b = 0;
+      GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kSortGroupThreads, 0));
+      kern<<<sm_count() * std::max(b, 1), kSortGroupThreads, 0, s>>>(c.row.p, lists.p + (uint64_t)cls * cap,
+                                                                      counts.p + cls, cap, c.adj.p);
       GARY_CUDA(cudaGetLastError());
-    }
-    const uint32_t nh = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
-                                                   thrust::counting_iterator<uint32_t>(n), big.p,
-                                                   RowLenIn{c.row.p, kSortCtaMax, 0xFFFFFFFFu}) - big.p);
+      return GARY_OK;
+    };
+    GARY_TRY(group_launch(k_sort_rows_group<1>, 0));
+    GARY_TRY(group_launch(k_sort_rows_group<2>, 1));
+    GARY_TRY(group_launch(k_sort_rows_group<3>, 2));
+    tr.mark("row sort: up to 8192 ids (warp groups)");
+    uint32_t nh = 0;
+    GARY_CUDA(cudaMemcpyAsync(&nh, counts.p + 3, 4, cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaStreamSynchronize(s));
     if (nh) {  // the longest rows (rare; d+ above 8192): one library radix sort per row
-      std::vector<uint32_t> hl(nh);
       std::vector<uint2> hr(nh);
       DevBuf<uint2> rr;
       GARY_TRY(rr.alloc(nh, s));
-      thrust::transform(pol, big.p, big.p + nh, rr.p, RowOf{c.row.p});
+      const uint32_t *l3 = lists.p + 3ull * cap;
+      thrust::transform(pol, l3, l3 + nh, rr.p, RowOf{c.row.p});
       GARY_CUDA(cudaMemcpyAsync(hr.data(), rr.p, (uint64_t)nh * 8, cudaMemcpyDeviceToHost, s));
       GARY_CUDA(cudaStreamSynchronize(s));
       uint32_t dmax = 0;
@@ -623,7 +772,7 @@ int ranked_dag_by_rows(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz
       }
     }
   }
-  tr.mark("row sort");
+  tr.mark("row sort: longer rows");
   GARY_TRY(wedge.alloc_persistent(n));
   k_rows_check_wedges<<<grid_for((uint64_t)n * 32), kThreads, 0, s>>>(
       c.row.p, c.adj.p, n, reinterpret_cast<unsigned long long *>(wedge.p), err);
