@@ -339,8 +339,8 @@ def run_ours(args, dist):
             if k > 0:  # first one warms the allocator
                 e2e_times.append(dt)
             assert res.value == count_local, "e2e count differs from the resident-graph count"
-        # the median step: host-to-device copies share the host's PCIe links with
-        # other jobs, whose bursts show up as single slow steps (the mean is reported too)
+        # the median step, with the mean and every step beside it: a rare step pays
+        # for a slow driver call on a host shared with other jobs
         e2e_s = dist.allreduce(statistics.median(e2e_times), "max")
         e2e_mean = dist.allreduce(sum(e2e_times) / len(e2e_times), "max")
         form = ("id-oriented DAG CSR, rows list neighbours v < u (the reference's csr_dag input)"

@@ -8,10 +8,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <exception>
+#include <iterator>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "graph.cuh"
@@ -84,15 +87,134 @@ cudaMemPool_t scratch_pool() {
   return g_pools[d];
 }
 
-void set_pool_keep_bytes(uint64_t bytes) {
-  std::lock_guard<std::mutex> lk(g_pool_mu);
-  g_pool_keep = bytes;
-  for (cudaMemPool_t p : g_pools) {
-    if (!p) continue;
-    uint64_t keep = bytes;
-    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
-    cudaMemPoolTrimTo(p, bytes);
+namespace {
+struct BlockInfo {
+  size_t bytes;
+  int dev;
+};
+std::mutex g_blk_mu;
+std::unordered_map<void *, BlockInfo> g_live;      // blocks handed out
+std::multimap<size_t, void *> g_cached[64];         // free blocks by rounded size, per device
+uint64_t g_cached_bytes[64] = {};
+
+size_t round_block(size_t b) {
+  if (b <= (1u << 20)) {
+    size_t r = 256;
+    while (r < b) r <<= 1;
+    return r;
   }
+  const size_t step = 2u << 20;
+  return (b + step - 1) / step * step;
+}
+
+// Returns cached blocks of device d to the driver, largest first, until at
+// most keep bytes stay cached.  Caller holds g_blk_mu.
+void trim_blocks_locked(int d, uint64_t keep) {
+  auto &c = g_cached[d];
+  if (c.empty() || g_cached_bytes[d] <= keep) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != d) cudaSetDevice(d);
+  while (g_cached_bytes[d] > keep && !c.empty()) {
+    auto it = std::prev(c.end());
+    cudaFree(it->second);
+    g_cached_bytes[d] -= it->first;
+    c.erase(it);
+  }
+  if (cur != d) cudaSetDevice(cur);
+}
+}  // namespace
+
+cudaError_t persistent_alloc(void **p, size_t bytes) {
+  const int d = device_ordinal();
+  const size_t rb = round_block(bytes);
+  if (d >= 0 && d < 64) {
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    auto &c = g_cached[d];
+    auto it = c.lower_bound(rb);
+    if (it != c.end() && it->first <= rb + rb / 8) {
+      *p = it->second;
+      g_live[*p] = BlockInfo{it->first, d};
+      g_cached_bytes[d] -= it->first;
+      c.erase(it);
+      return cudaSuccess;
+    }
+  }
+  cudaError_t e = cudaMalloc(p, rb);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    release_cached_memory();
+    e = cudaMalloc(p, rb);
+  }
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_blk_mu);
+  g_live[*p] = BlockInfo{rb, d};
+  return cudaSuccess;
+}
+
+void persistent_free(void *p) {
+  BlockInfo info{0, -1};
+  {
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    auto it = g_live.find(p);
+    if (it != g_live.end()) {
+      info = it->second;
+      g_live.erase(it);
+    }
+  }
+  if (info.dev < 0 || info.dev >= 64) {
+    cudaFree(p);
+    return;
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != info.dev) cudaSetDevice(info.dev);
+  if (cudaDeviceSynchronize() != cudaSuccess) cudaGetLastError();
+  {
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    g_cached[info.dev].emplace(info.bytes, p);
+    g_cached_bytes[info.dev] += info.bytes;
+    uint64_t keep;
+    {
+      std::lock_guard<std::mutex> lk2(g_pool_mu);
+      keep = g_pool_keep;
+    }
+    trim_blocks_locked(info.dev, keep);
+  }
+  if (cur != info.dev) cudaSetDevice(cur);
+}
+
+void release_cached_memory() {
+  {
+    std::lock_guard<std::mutex> lk(g_blk_mu);
+    for (int d = 0; d < 64; ++d) trim_blocks_locked(d, 0);
+  }
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (int d = 0; d < 64; ++d) {
+    if (!g_pools[d]) continue;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != d) cudaSetDevice(d);
+    cudaDeviceSynchronize();
+    cudaMemPoolTrimTo(g_pools[d], 0);
+    if (cur != d) cudaSetDevice(cur);
+  }
+  cudaGetLastError();
+}
+
+void set_pool_keep_bytes(uint64_t bytes) {
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    g_pool_keep = bytes;
+    for (cudaMemPool_t p : g_pools) {
+      if (!p) continue;
+      uint64_t keep = bytes;
+      cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+      cudaMemPoolTrimTo(p, bytes);
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_blk_mu);
+  for (int d = 0; d < 64; ++d) trim_blocks_locked(d, bytes);
 }
 
 namespace {

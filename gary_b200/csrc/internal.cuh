@@ -54,6 +54,21 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 cudaMemPool_t scratch_pool();
 void set_pool_keep_bytes(uint64_t bytes);
 
+// ---- cached blocks for arrays that outlive a call -------------------------
+// persistent_alloc hands out a cudaMalloc'd block (sizes rounded up: powers of
+// two to 1 MiB, then 2 MiB steps), reusing a cached block of the same rounded
+// size (up to 1/8 larger) when one is free.  persistent_free synchronises the
+// block's device, as cudaFree does, so that no kernel still in flight can use
+// the block, and then keeps it for the next allocation instead of returning
+// it to the driver: an upload that follows a free of a graph of the same
+// shape makes no driver allocation call at all.  The cache shares the
+// "pool_keep_bytes" limit with the scratch pool.  An allocation that finds
+// the device full empties the cache and the scratch pool's free pages and
+// tries once more.
+cudaError_t persistent_alloc(void **p, size_t bytes);
+void persistent_free(void *p);
+void release_cached_memory();
+
 // ---- phase trace (GARY_TRACE=1 in the environment) -----------------------
 // mark() synchronises the stream and prints the wall time since the previous
 // mark to stderr; with tracing off it does nothing and costs nothing.
@@ -69,8 +84,9 @@ struct PhaseTrace {
 
 // ---- device buffer with RAII --------------------------------------------
 // alloc(): stream-ordered temporary from the scratch pool (freed on the same
-// stream).  alloc_persistent(): cudaMalloc / cudaFree, for arrays that outlive
-// the call and so must not depend on the caller's stream.
+// stream).  alloc_persistent(): a cached block (persistent_alloc /
+// persistent_free), for arrays that outlive the call and so must not depend
+// on the caller's stream.
 template <typename T>
 struct DevBuf {
   T *p = nullptr;
@@ -95,7 +111,7 @@ struct DevBuf {
   void release() {
     if (p) {
       if (async) cudaFreeAsync(p, s);
-      else cudaFree(p);
+      else persistent_free(p);
     }
     p = nullptr;
     n = 0;
@@ -112,7 +128,12 @@ struct DevBuf {
     cudaError_t e = is_async
         ? cudaMallocFromPoolAsync(reinterpret_cast<void **>(&p), count * sizeof(T),
                                   scratch_pool(), stream)
-        : cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T));
+        : persistent_alloc(reinterpret_cast<void **>(&p), count * sizeof(T));
+    if (e == cudaErrorMemoryAllocation && is_async) {  // cached blocks may hold the room
+      cudaGetLastError();
+      release_cached_memory();
+      e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(&p), count * sizeof(T), scratch_pool(), stream);
+    }
     if (e != cudaSuccess) {
       p = nullptr;
       n = 0;

@@ -212,11 +212,13 @@ int gary_gen_ba(uint32_t n, uint32_t m, uint64_t seed, uint32_t *src, uint32_t *
  *   "vertex_overhead" fixed cost charged per vertex      (default 64)
  *   "min_blocks"      resident CTAs per SM, 2 or 3; 0 (the default) picks 3
  *                     from 2^31 probes on, else 2
- *   "pool_keep_bytes" freed construction scratch the library's per-device
- *                     memory pool keeps mapped across syncs (default
- *                     UINT64_MAX: all of it, like a caching allocator; 0
- *                     trims the pool now and hands scratch back at every
- *                     sync); "reset" leaves it alone
+ *   "pool_keep_bytes" freed device memory the library keeps for reuse, per
+ *                     device and per kind: construction scratch in its
+ *                     memory pool across syncs, and the blocks of freed
+ *                     graphs and plans (default UINT64_MAX: all of it, like
+ *                     a caching allocator, so a repeated upload makes no
+ *                     driver allocation call; 0 returns both now and at
+ *                     every later free or sync); "reset" leaves it alone
  *   "reset"           restore every plan default
  * No reference counterpart: the reference fixes its launch shape in each test
  * (test/TriQueryTest.cu:98-99, 116-117). */
