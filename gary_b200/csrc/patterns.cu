@@ -205,8 +205,16 @@ __global__ void __launch_bounds__(kMidThreads, 1)
 }
 
 // ---- C4, heavy vertices: dense counters over windows of w ids ---------------
-constexpr uint32_t kWinWords = 48 * 1024;  // counters per window: 192 KiB of shared memory
-constexpr int kWinThreads = 1024;
+// A window is kWinIds consecutive w ids; its counters take kWinWords shared
+// words (96 KiB), so two 512-thread CTAs share an SM and one runs while the
+// other waits at a barrier.  A counter never exceeds pre(u), the number of
+// lower neighbours of u, so for pre(u) < 2^16 two 16-bit counters share a
+// word and a whole window fits; otherwise the window is counted in two
+// halves of kWinWords 32-bit counters.
+constexpr uint32_t kWinIds = 48 * 1024;
+constexpr uint32_t kWinWords = 24 * 1024;
+constexpr uint32_t kWin16MaxPre = 0xFFFFu;
+constexpr int kWinThreads = 512;
 constexpr int kWinWarps = kWinThreads / 32;
 
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *l, uint32_t b, uint32_t e,
@@ -231,6 +239,29 @@ __device__ __forceinline__ uint32_t gallop_geq(const uint32_t *l, uint32_t c, ui
   }
   const uint64_t e = (uint64_t)b + step < len ? (uint64_t)b + step : len;
   return lower_bound_u32(l, b + 1, (uint32_t)e, x);
+}
+
+// The same answer for a list in the padded layout (32-byte aligned, padded
+// with kSentinel to a multiple of 8): the 16 ids of the two octets from c's
+// octet come in one round of loads and settle most runs (70 % of a window's
+// runs hold at most 8 ids); only a run that goes past them gallops on.
+__device__ __forceinline__ uint32_t run_end(const uint32_t *l, uint32_t c, uint32_t len, uint32_t x) {
+  if (c >= len) return c;
+  const uint32_t ob = c & ~7u;
+  const uint32_t plen = (len + 7u) & ~7u;
+  const uint4 *q = reinterpret_cast<const uint4 *>(l + ob);
+  const uint4 s4 = make_uint4(kSentinel, kSentinel, kSentinel, kSentinel);
+  const uint4 a0 = q[0], a1 = q[1];
+  const bool two = ob + 8 < plen;
+  const uint4 b0 = two ? q[2] : s4, b1 = two ? q[3] : s4;
+  const uint32_t id[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
+                           b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+  uint32_t e = kSentinel;
+#pragma unroll
+  for (int i = 15; i >= 0; --i)
+    if (ob + i >= c && (ob + i >= len || id[i] >= x)) e = ob + i;
+  if (e != kSentinel) return e;
+  return gallop_geq(l, ob + 16, len, x);  // ids [c, ob + 16) are all below x
 }
 
 __device__ __forceinline__ uint32_t warp_min_u32(uint32_t x) {
@@ -258,15 +289,17 @@ __device__ __forceinline__ void walk_ranges(const uint32_t *__restrict__ adj, ui
 }
 
 // Tile {v0 = u, v1 = pre, j0 = wa, j1 = wb}: windows [wa, wb) of vertex u,
-// i.e. wedge ends w in [wa * kWinWords, min(wb * kWinWords, u)).
+// i.e. wedge ends w in [wa * kWinIds, min(wb * kWinIds, u)).  The kernel
+// steps through them in passes of ws ids: kWinIds with 16-bit counters,
+// kWinIds / 2 with 32-bit ones.
 //
 // Per lower neighbour k (v = N(u)[k]) the CTA keeps, in its HBM scratch, v's
-// row record, a cursor into N(v), the cursor before the last window, and the
-// window index of the id at the cursor (nextw).  A window pass scans nextw,
-// compacts the neighbours whose next id falls in the window into an active
-// list, and only those gallop and walk; the pass also yields the next
-// non-empty window.  Neighbours with few ids below u are active in few
-// windows, so most passes touch a small part of the list.
+// row record, a cursor into N(v), the cursor before the last pass, and the
+// pass index of the id at the cursor (nextw).  A pass scans nextw, compacts
+// the neighbours whose next id falls in it into an active list, and only
+// those walk; the scan also yields the next non-empty pass.  Neighbours with
+// few ids below u are active in few passes, so most passes touch a small part
+// of the list.
 constexpr uint32_t kNoWindow = 0xFFFFFFFFu;
 
 struct C4Scratch {
@@ -287,11 +320,19 @@ __device__ __forceinline__ C4Scratch c4_scratch(uint32_t *base, uint32_t max_pre
 // words of scratch per lower neighbour (vrow 2, cur, prev, nextw, act)
 constexpr uint32_t kC4ScratchWords = 6;
 
-__global__ void __launch_bounds__(kWinThreads)
+// Counter of w (offset o = w - lo in the pass) incremented; returns its old value.
+template <bool WIDE>
+__device__ __forceinline__ uint32_t win_incr(uint32_t *cnt, uint32_t o) {
+  if (WIDE) return atomicAdd(&cnt[o], 1u);
+  const uint32_t sh = (o & 1u) << 4;
+  return (atomicAdd(&cnt[o >> 1], 1u << sh) >> sh) & 0xFFFFu;
+}
+
+__global__ void __launch_bounds__(kWinThreads, 2)
     k_c4_win(GraphView s, const Tile *__restrict__ tiles, uint32_t t_lo, uint32_t t_hi,
              uint32_t *__restrict__ scratch, uint32_t max_pre, SchedState *sched,
              unsigned long long *__restrict__ out) {
-  extern __shared__ __align__(16) uint32_t cnt[];  // kWinWords counters, zero between windows
+  extern __shared__ __align__(16) uint32_t cnt[];  // kWinWords words, zero between passes
   __shared__ uint32_t s_tile, s_next, s_nact, s_minw;
   __shared__ unsigned long long s_wedges;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -308,18 +349,20 @@ __global__ void __launch_bounds__(kWinThreads)
     if (t >= t_hi) break;
     const Tile tl = tiles[t];
     const uint32_t u = tl.v0, pre = tl.v1;
+    const bool wide = pre > kWin16MaxPre;
+    const uint32_t ws = wide ? kWinIds / 2 : kWinIds;  // ids per pass
     const uint32_t *au = s.adj + (uint64_t)s.row[u].x * 4;
-    const uint64_t end64 = (uint64_t)tl.j1 * kWinWords, begin64 = (uint64_t)tl.j0 * kWinWords;
+    const uint64_t end64 = (uint64_t)tl.j1 * kWinIds, begin64 = (uint64_t)tl.j0 * kWinIds;
     const uint32_t w_end = end64 < u ? (uint32_t)end64 : u;
     const uint32_t w_begin = begin64 < w_end ? (uint32_t)begin64 : w_end;
-    // state at the tile's first window
+    // state at the tile's first pass
     uint32_t mw = kNoWindow;
     for (uint32_t k = threadIdx.x; k < pre; k += blockDim.x) {
       const uint2 rv = s.row[au[k]];
       const uint32_t *l = s.adj + (uint64_t)rv.x * 4;
       const uint32_t c = lower_bound_u32(l, 0, rv.y, w_begin);
       const uint32_t x = c < rv.y ? l[c] : kSentinel;
-      const uint32_t nw = x < w_end ? x / kWinWords : kNoWindow;
+      const uint32_t nw = x < w_end ? x / ws : kNoWindow;
       cs.vrow[k] = rv;
       cs.cur[k] = c;
       cs.nextw[k] = nw;
@@ -331,8 +374,8 @@ __global__ void __launch_bounds__(kWinThreads)
     while (true) {
       const uint32_t win = s_minw;
       if (win == kNoWindow) break;  // no id of the tile's range is left
-      const uint32_t lo = win * kWinWords;
-      const uint32_t hi = lo + kWinWords < w_end ? lo + kWinWords : w_end;
+      const uint32_t lo = win * ws;
+      const uint32_t hi = lo + ws < w_end ? lo + ws : w_end;
       __syncthreads();  // every thread has read s_minw
       if (threadIdx.x == 0) {
         s_next = 0;
@@ -341,18 +384,24 @@ __global__ void __launch_bounds__(kWinThreads)
         s_wedges = 0;
       }
       __syncthreads();
-      // active neighbours of this window; the others keep their next window
+      // active neighbours of this pass; the others keep their next pass
       uint32_t mwi = kNoWindow;
-      for (uint32_t k = threadIdx.x; k < pre; k += blockDim.x) {
-        const uint32_t nw = cs.nextw[k];
-        if (nw == win) cs.act[atomicAdd(&s_nact, 1u)] = k;
+      for (uint32_t k0 = warp * 32; k0 < pre; k0 += kWinThreads) {
+        const uint32_t k = k0 + lane;
+        const uint32_t nw = k < pre ? cs.nextw[k] : kNoWindow;
+        const bool on = nw == win;
+        const unsigned m = __ballot_sync(kFull, on);
+        uint32_t at = 0;
+        if (lane == 0 && m) at = atomicAdd(&s_nact, (uint32_t)__popc(m));
+        at = __shfl_sync(kFull, at, 0);
+        if (on) cs.act[at + __popc(m & ((1u << lane) - 1u))] = k;
         else mwi = min(mwi, nw);
       }
       mwi = warp_min_u32(mwi);
       if (lane == 0) atomicMin(&s_minw, mwi);
       __syncthreads();
       const uint32_t nact = s_nact;
-      // count: advance the active cursors past the window, counting the ids passed
+      // count: advance the active cursors past the pass, counting the ids passed
       uint32_t nxt = kNoWindow;
       unsigned long long seen = 0;
       while (true) {
@@ -367,17 +416,20 @@ __global__ void __launch_bounds__(kWinThreads)
           const uint2 rv = cs.vrow[k];
           const uint32_t *l = s.adj + (uint64_t)rv.x * 4;
           b = cs.cur[k];
-          e = gallop_geq(l, b, rv.y, hi);
+          e = run_end(l, b, rv.y, hi);
           cs.prev[k] = b;
           cs.cur[k] = e;
           const uint32_t x = e < rv.y ? l[e] : kSentinel;
-          const uint32_t nw = x < w_end ? x / kWinWords : kNoWindow;
+          const uint32_t nw = x < w_end ? x / ws : kNoWindow;
           cs.nextw[k] = nw;
           nxt = min(nxt, nw);
           q4 = rv.x;
           seen += e - b;
         }
-        walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { acc += atomicAdd(&cnt[w - lo], 1u); });
+        if (wide)
+          walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { acc += win_incr<true>(cnt, w - lo); });
+        else
+          walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { acc += win_incr<false>(cnt, w - lo); });
       }
       nxt = warp_min_u32(nxt);
       seen = warp_sum_u64(seen);
@@ -386,8 +438,9 @@ __global__ void __launch_bounds__(kWinThreads)
         if (seen) atomicAdd(&s_wedges, seen);
       }
       __syncthreads();
-      // zero the window again: walk the same ids when few, else clear it whole
-      if (s_wedges + nact < (hi - lo) / 4) {
+      // zero the pass's counters again: walk the same ids when few, else clear them whole
+      const uint32_t words = wide ? hi - lo : (hi - lo + 1) >> 1;
+      if (s_wedges + nact < words / 4) {
         for (uint32_t a0 = warp * 32; a0 < nact; a0 += kWinWarps * 32) {
           const uint32_t a = a0 + lane;
           uint32_t q4 = 0, b = 0, e = 0;
@@ -397,10 +450,10 @@ __global__ void __launch_bounds__(kWinThreads)
             b = cs.prev[k];
             e = cs.cur[k];
           }
-          walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { cnt[w - lo] = 0u; });
+          walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { cnt[wide ? w - lo : (w - lo) >> 1] = 0u; });
         }
       } else {
-        for (uint32_t i = threadIdx.x; i < hi - lo; i += blockDim.x) cnt[i] = 0;
+        for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) cnt[i] = 0;
       }
       __syncthreads();
     }
@@ -618,7 +671,7 @@ __global__ void k_c4_exact_wedges(const uint2 *__restrict__ srow, const uint32_t
 }
 
 __host__ __device__ __forceinline__ uint32_t c4_windows(uint32_t u) {
-  return (uint32_t)(((uint64_t)u + kWinWords - 1) / kWinWords);
+  return (uint32_t)(((uint64_t)u + kWinIds - 1) / kWinIds);
 }
 
 // Cost of a heavy vertex in probe units: its wedges, a cursor step per
