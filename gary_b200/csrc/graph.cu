@@ -839,6 +839,52 @@ __global__ void k_gather_u32(const uint32_t *__restrict__ perm, const uint32_t *
 // group_off (host, ngroups + 1 entries; may be null): vertices
 // [group_off[g], group_off[g+1]) form graph g of a disjoint union.  Ranks are
 // then taken within each graph, so every graph keeps a contiguous rank range.
+// Host ids copied in chunks on a side stream, so that the upload's stream can
+// run what needs only the offsets while they cross PCIe.  wait(k) makes the
+// upload's stream wait for chunk k; the destructor makes it wait for every
+// chunk, so a stream-ordered free of the destination on that stream (error
+// paths included) never overtakes a copy.
+struct ChunkedCopy {
+  static constexpr int kMaxChunks = 8;
+  cudaStream_t s = nullptr, side = nullptr;
+  cudaEvent_t done[kMaxChunks] = {};
+  uint64_t off[kMaxChunks + 1] = {};
+  int chunks = 0;
+  ChunkedCopy() = default;
+  ChunkedCopy(const ChunkedCopy &) = delete;
+  ChunkedCopy &operator=(const ChunkedCopy &) = delete;
+  int start(uint32_t *dst, const uint32_t *src, uint64_t count, cudaStream_t stream) {
+    s = stream;
+    GARY_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    cudaEvent_t ready;
+    GARY_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    cudaEventRecord(ready, s);  // dst was allocated on s
+    cudaStreamWaitEvent(side, ready, 0);
+    cudaEventDestroy(ready);
+    const uint64_t min_chunk = 1ull << 24;  // ids
+    chunks = (int)std::min<uint64_t>(kMaxChunks, std::max<uint64_t>(1, count / min_chunk));
+    for (int k = 0; k <= chunks; ++k) off[k] = count * (uint64_t)k / (uint64_t)chunks;
+    for (int k = 0; k < chunks; ++k) {
+      GARY_CUDA(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+      GARY_CUDA(cudaMemcpyAsync(dst + off[k], src + off[k], (off[k + 1] - off[k]) * 4,
+                                cudaMemcpyHostToDevice, side));
+      GARY_CUDA(cudaEventRecord(done[k], side));
+    }
+    return GARY_OK;
+  }
+  void wait(int k) const {
+    if (k < chunks && done[k]) cudaStreamWaitEvent(s, done[k], 0);
+  }
+  ~ChunkedCopy() {
+    for (int k = 0; k < chunks; ++k)
+      if (done[k]) {
+        cudaStreamWaitEvent(s, done[k], 0);
+        cudaEventDestroy(done[k]);
+      }
+    if (side) cudaStreamDestroy(side);
+  }
+};
+
 int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, uint32_t flags,
            cudaStream_t s, gary_graph **out, const uint64_t *group_off, uint32_t ngroups) {
   const bool on_dev = flags & GARY_INPUT_DEVICE;
@@ -862,22 +908,27 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   auto pol = thrust::cuda::par_nosync.on(s);
   PhaseTrace tr("upload", s);
 
-  // 1. input on the device
+  // 1. input on the device.  From host memory the offsets come first on s and
+  // the ids in chunks on a side stream; s meanwhile derives what needs only
+  // the offsets (degrees of symmetric input, row ids, and for symmetric input
+  // the ranks too) and, for DAG input, counts in-degrees chunk by chunk.
   DevBuf<uint64_t> dptr_own;
   DevBuf<uint32_t> didx_own;
   const uint64_t *dptr = ptr;
   const uint32_t *didx = idx;
+  ChunkedCopy ids;  // after didx_own: destroyed first, so s waits for the copies before the free
   if (!on_dev) {
     GARY_TRY(dptr_own.alloc((uint64_t)n + 1, s));
     GARY_TRY(didx_own.alloc(nnz, s));
     GARY_CUDA(cudaMemcpyAsync(dptr_own.p, ptr, ((uint64_t)n + 1) * 8, cudaMemcpyHostToDevice, s));
-    if (nnz)
-      GARY_CUDA(cudaMemcpyAsync(didx_own.p, idx, nnz * 4, cudaMemcpyHostToDevice, s));
+    if (nnz) GARY_TRY(ids.start(didx_own.p, idx, nnz, s));
     dptr = dptr_own.p;
     didx = didx_own.p;
   }
+  auto wait_ids = [&] {
+    for (int k = 0; k < ids.chunks; ++k) ids.wait(k);
+  };
 
-  tr.mark("h2d input");
   DevBuf<unsigned> err;
   GARY_TRY(err.alloc(1, s));
   GARY_CUDA(cudaMemsetAsync(err.p, 0, sizeof(unsigned), s));
@@ -886,7 +937,30 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   DevBuf<uint32_t> deg;
   GARY_TRY(deg.alloc(n, s));
   k_degree<<<grid_for(n), kThreads, 0, s>>>(dptr, n, nnz, deg.p, err.p);
-  if (dag && nnz) k_indegree<<<grid_for(nnz), kThreads, 0, s>>>(didx, nnz, n, deg.p, err.p);
+  // row id of every entry: heads, then an inclusive max-scan (offsets only)
+  const int lg = bits_for(n);
+  DevBuf<uint32_t> rowid;
+  GARY_TRY(rowid.alloc(nnz, s));
+  if (nnz) {
+    GARY_CUDA(cudaMemsetAsync(rowid.p, 0, nnz * 4, s));
+    k_row_heads<<<grid_for(n), kThreads, 0, s>>>(dptr, n, rowid.p);
+    size_t tmp = 0;
+    GARY_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
+    DevBuf<uint8_t> t;
+    GARY_TRY(t.alloc(tmp, s));
+    GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
+  }
+  if (dag && nnz) {
+    if (ids.chunks) {
+      for (int k = 0; k < ids.chunks; ++k) {
+        ids.wait(k);
+        const uint64_t len = ids.off[k + 1] - ids.off[k];
+        k_indegree<<<grid_for(len), kThreads, 0, s>>>(didx + ids.off[k], len, n, deg.p, err.p);
+      }
+    } else {
+      k_indegree<<<grid_for(nnz), kThreads, 0, s>>>(didx, nnz, n, deg.p, err.p);
+    }
+  }
   GARY_CUDA(cudaGetLastError());
   if (on_dev) {
     uint64_t ends[2];
@@ -897,7 +971,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   }
   g->max_degree = thrust::reduce(pol, deg.p, deg.p + n, 0u, MaxU32());
 
-  tr.mark("degrees");
+  tr.mark("h2d offsets, degrees, row ids");
   // 3. ranks by (graph, degree, id): a stable radix sort of the ids
   DevBuf<uint32_t> rank, gidc;
   if (ngroups) {
@@ -944,21 +1018,9 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   }
 
   tr.mark("ranks");
-  // 4. row id of every entry: heads, then an inclusive max-scan
-  const int lg = bits_for(n);
-  DevBuf<uint32_t> rowid;
-  GARY_TRY(rowid.alloc(nnz, s));
-  if (nnz) {
-    GARY_CUDA(cudaMemsetAsync(rowid.p, 0, nnz * 4, s));
-    k_row_heads<<<grid_for(n), kThreads, 0, s>>>(dptr, n, rowid.p);
-    size_t tmp = 0;
-    GARY_CUDA(cub::DeviceScan::InclusiveScan(nullptr, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
-    DevBuf<uint8_t> t;
-    GARY_TRY(t.alloc(tmp, s));
-    GARY_CUDA(cub::DeviceScan::InclusiveScan(t.p, tmp, rowid.p, rowid.p, MaxU32(), nnz, s));
-  }
-
-  tr.mark("row ids");
+  // 4. the ids themselves from here on
+  wait_ids();
+  tr.mark("h2d ids (rest)");
   // 5. the ranked DAG's padded lists, validated; per-vertex wedge counts
   uint64_t m = 0;
   GARY_TRY(ranked_dag_by_rows(rowid.p, didx, nnz, n, deg.p, rank.p, dag, validate, err.p, g->dag,

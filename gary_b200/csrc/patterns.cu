@@ -26,7 +26,8 @@
 //   light  (<= 512)    a warp's shared hash map;
 //   medium (<= 8192)   a CTA's shared hash map;
 //   heavy              dense counters in shared memory over windows of
-//                      48 K consecutive w ids.  Each v keeps a cursor into
+//                      32 K consecutive w ids (16-bit counters, two to a
+//                      word, three CTAs per SM).  Each v keeps a cursor into
 //                      N(v) (sorted), so a window pass reads exactly the ids
 //                      that fall in it; windows nothing reaches are skipped,
 //                      and a heavy u is cut into tiles of consecutive windows
@@ -206,13 +207,15 @@ __global__ void __launch_bounds__(kMidThreads, 1)
 
 // ---- C4, heavy vertices: dense counters over windows of w ids ---------------
 // A window is kWinIds consecutive w ids; its counters take kWinWords shared
-// words (96 KiB), so two 512-thread CTAs share an SM and one runs while the
-// other waits at a barrier.  A counter never exceeds pre(u), the number of
-// lower neighbours of u, so for pre(u) < 2^16 two 16-bit counters share a
-// word and a whole window fits; otherwise the window is counted in two
-// halves of kWinWords 32-bit counters.
-constexpr uint32_t kWinIds = 48 * 1024;
-constexpr uint32_t kWinWords = 24 * 1024;
+// words (64 KiB), so three 512-thread CTAs share an SM and the others run
+// while one waits at a barrier (measured at RMAT-22 / RMAT-24: 48 K ids with
+// two CTAs per SM 260 ms / 5.53 s, 32 K ids with three 225 ms / 4.88 s,
+// 24 K ids with four 256-thread CTAs 317 ms / 7.57 s).  A counter never
+// exceeds pre(u), the number of lower neighbours of u, so for pre(u) < 2^16
+// two 16-bit counters share a word and a whole window fits; otherwise the
+// window is counted in two halves of kWinWords 32-bit counters.
+constexpr uint32_t kWinIds = 32 * 1024;
+constexpr uint32_t kWinWords = 16 * 1024;
 constexpr uint32_t kWin16MaxPre = 0xFFFFu;
 constexpr int kWinThreads = 512;
 constexpr int kWinWarps = kWinThreads / 32;
@@ -328,7 +331,7 @@ __device__ __forceinline__ uint32_t win_incr(uint32_t *cnt, uint32_t o) {
   return (atomicAdd(&cnt[o >> 1], 1u << sh) >> sh) & 0xFFFFu;
 }
 
-__global__ void __launch_bounds__(kWinThreads, 2)
+__global__ void __launch_bounds__(kWinThreads, 3)
     k_c4_win(GraphView s, const Tile *__restrict__ tiles, uint32_t t_lo, uint32_t t_hi,
              uint32_t *__restrict__ scratch, uint32_t max_pre, SchedState *sched,
              unsigned long long *__restrict__ out) {
