@@ -559,10 +559,12 @@ int row_starts(const DevBuf<uint64_t> &keys, uint64_t m, uint32_t n, int lg,
   if (persistent) GARY_TRY(rowstart.alloc_persistent((uint64_t)n + 1));
   else GARY_TRY(rowstart.alloc((uint64_t)n + 1, s));
   // fill with m, heads, then reverse min-scan so empty rows point at the next row
-  thrust::fill(thrust::cuda::par_nosync.on(s), rowstart.p, rowstart.p + n + 1, m);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
+  thrust::fill(pol, rowstart.p, rowstart.p + n + 1, m);
   if (m) k_key_heads<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, lg, rowstart.p);
   auto rb = thrust::make_reverse_iterator(rowstart.p + n + 1);
-  thrust::inclusive_scan(thrust::cuda::par_nosync.on(s), rb, rb + n + 1, rb, MinU64());
+  thrust::inclusive_scan(pol, rb, rb + n + 1, rb, MinU64());
   GARY_CUDA(cudaGetLastError());
   return GARY_OK;
 }
@@ -630,7 +632,8 @@ int unique_keys(DevBuf<uint64_t> &keys, uint64_t count, uint64_t &kept, cudaStre
 // Padded lists from sorted (row << lg | col) keys.
 int padded_from_keys(const DevBuf<uint64_t> &keys, uint64_t m, uint32_t n, int lg, PaddedCSR &c,
                      cudaStream_t s) {
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   c.n = n;
   c.m = m;
   DevBuf<uint64_t> rowstart, off4;
@@ -666,7 +669,8 @@ int ranked_dag_by_rows(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz
                        const uint32_t *deg, const uint32_t *rank, bool dag, bool validate,
                        unsigned *err, PaddedCSR &c, DevBuf<uint64_t> &wedge, uint64_t &m,
                        cudaStream_t s) {
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   PhaseTrace tr("dag rows", s);
   c.n = n;
   GARY_TRY(c.outdeg.alloc_persistent(n));
@@ -790,7 +794,8 @@ int ranked_dag_by_rows(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz
 int oriented_keys(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz, uint32_t n,
                   const uint32_t *deg, const uint32_t *rank, int lg, bool dag, bool validate,
                   unsigned *err, DevBuf<uint64_t> &keys, uint64_t &m, cudaStream_t s) {
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   m = 0;
   GARY_TRY(keys.alloc(std::max<uint64_t>(nnz, 1), s));
   if (nnz) {
@@ -905,7 +910,8 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
   g->n = n;
   g->flags = flags;
   g->keep_ids = keep_ids;
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   PhaseTrace tr("upload", s);
 
   // 1. input on the device.  From host memory the offsets come first on s and
@@ -995,7 +1001,7 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
     GARY_TRY(dk.alloc(n, s));
     GARY_TRY(dk2.alloc(n, s));
     GARY_TRY(g->perm.alloc_persistent(n));
-    GARY_TRY(perm2.alloc_persistent(n));
+    GARY_TRY(perm2.alloc(n, s));  // scratch: releasing a persistent block synchronises the device
     k_rank_keys<<<grid_for(n), kThreads, 0, s>>>(deg.p, ngroups ? gidc.p : nullptr, n, degbits, dk.p);
     thrust::sequence(pol, perm2.p, perm2.p + n, 0u);
     cub::DoubleBuffer<uint64_t> kb(dk.p, dk2.p);
@@ -1005,7 +1011,8 @@ int upload(const uint64_t *ptr, const uint32_t *idx, uint32_t n, uint64_t nnz, u
     DevBuf<uint8_t> t;
     GARY_TRY(t.alloc(tmp, s));
     GARY_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kb, vb, n, 0, keybits, s));
-    if (vb.Current() != g->perm.p) std::swap(g->perm, perm2);
+    if (vb.Current() != g->perm.p)
+      GARY_CUDA(cudaMemcpyAsync(g->perm.p, vb.Current(), (uint64_t)n * 4, cudaMemcpyDeviceToDevice, s));
     GARY_TRY(rank.alloc(n, s));
     GARY_TRY(g->rdeg.alloc_persistent(n));
     k_rank_scatter<<<grid_for(n), kThreads, 0, s>>>(g->perm.p, deg.p, n, rank.p, g->rdeg.p);
@@ -1085,7 +1092,8 @@ int csr_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t m, uint32_
   auto c = std::make_unique<gary_csr>();
   GARY_CUDA(cudaGetDevice(&c->device));
   c->n = n;
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   const int lg = bits_for(n);
   DevBuf<uint32_t> s_own, d_own;
   if (!(flags & GARY_INPUT_DEVICE) && m) {
@@ -1174,7 +1182,8 @@ int padded_rowid(const PaddedCSR &c, DevBuf<uint32_t> &rowid, cudaStream_t s) {
 
 int build_coo(PaddedCSR &c, cudaStream_t s) {
   if (c.coo_row.p || c.m == 0) return GARY_OK;
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   DevBuf<uint32_t> rowid;
   GARY_TRY(padded_rowid(c, rowid, s));
   DevBuf<uint64_t> words, nsel;
@@ -1229,7 +1238,8 @@ __global__ void k_sym_keys(const uint2 *__restrict__ row, const uint32_t *__rest
 // Symmetric lists in rank ids (for 4-cycle counting), built once on demand.
 int build_symmetric(gary_graph *g, cudaStream_t s) {
   if (g->sym.row.p) return GARY_OK;
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   const uint32_t n = g->n;
   const int lg = bits_for(n);
   const uint64_t W = g->dag.words;

@@ -2,7 +2,9 @@
 #pragma once
 #include <cstdarg>
 #include <cstdint>
+#include <cstddef>
 #include <cstdio>
+#include <new>
 #include <cuda_runtime.h>
 
 #include "gary_b200.h"
@@ -54,6 +56,27 @@ inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s
 cudaMemPool_t scratch_pool();
 void set_pool_keep_bytes(uint64_t bytes);
 
+// Thrust temporaries from the scratch pool, stream-ordered on s.  Thrust's
+// default allocator calls cudaMalloc / cudaFree, and cudaFree synchronises the
+// whole device (a copy in flight on another stream included).  Use as
+//   ScratchAlloc pol_alloc{s};
+//   auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
+// A failed allocation throws std::bad_alloc, which the C-ABI entry points
+// turn into GARY_ERR_OOM.
+struct ScratchAlloc {
+  using value_type = char;
+  cudaStream_t s;
+  char *allocate(std::ptrdiff_t n) {
+    void *p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, (size_t)n, scratch_pool(), s) != cudaSuccess) {
+      cudaGetLastError();
+      throw std::bad_alloc();
+    }
+    return static_cast<char *>(p);
+  }
+  void deallocate(char *p, size_t) { cudaFreeAsync(p, s); }
+};
+
 // ---- cached blocks for arrays that outlive a call -------------------------
 // persistent_alloc hands out a cudaMalloc'd block (sizes rounded up: powers of
 // two to 1 MiB, then 2 MiB steps), reusing a cached block of the same rounded
@@ -61,7 +84,8 @@ void set_pool_keep_bytes(uint64_t bytes);
 // block's device, as cudaFree does, so that no kernel still in flight can use
 // the block, and then keeps it for the next allocation instead of returning
 // it to the driver: an upload that follows a free of a graph of the same
-// shape makes no driver allocation call at all.  The cache shares the
+// shape makes no driver allocation call at all.  Because a free synchronises
+// the device, temporaries inside a call come from the scratch pool instead.  The cache shares the
 // "pool_keep_bytes" limit with the scratch pool.  An allocation that finds
 // the device full empties the cache and the scratch pool's free pages and
 // tries once more.

@@ -764,7 +764,8 @@ int c4_win_attr() {
 int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
   auto plan = std::make_unique<PatternPlan>();
   const uint32_t n = g->n;
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   const uint32_t *dp = g->dag.outdeg.p;
   // warp and mid vertices in id order; big vertices largest first
   GARY_TRY(plan->light.alloc_persistent(std::max<uint32_t>(n, 1)));
@@ -862,7 +863,8 @@ int build_c4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
   GARY_TRY(build_symmetric(g, s));
   auto plan = std::make_unique<PatternPlan>();
   const uint32_t n = g->n;
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   DevBuf<uint8_t> cls;
   GARY_TRY(cls.alloc(n, s));
   k_c4_classify<<<grid_for(n), kThreads, 0, s>>>(g->sym.row.p, g->sym.adj.p, g->dag.outdeg.p, n,

@@ -306,7 +306,8 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
     set_error("graph too large for the in-edge index (%llu padded words)", (unsigned long long)W);
     return GARY_ERR_UNSUPPORTED;
   }
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   DevBuf<uint32_t> keys, keys2;
   DevBuf<uint2> vals, vals2;
   {
@@ -386,7 +387,8 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp_in, cudaStream_t s, gary_c
                   const float *model) {
   auto plan = std::make_unique<gary_count_plan>();
   const uint32_t n = g->n;
-  auto pol = thrust::cuda::par_nosync.on(s);
+  ScratchAlloc pol_alloc{s};
+  auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   PhaseTrace tr("triangle plan", s);
   GARY_TRY(build_in_index(g, s, plan->in));
   tr.mark("in-edge index");
