@@ -79,3 +79,35 @@ def test_c4_trace_identity_on_gpu(cuda):
     with gb.Graph.upload(ptr, idx, 1 << 12) as g:
         c4 = g.count(C4)
     assert O.c4_hom(ptr, idx) == 8 * c4 + 2 * int((d * (d - 1)).sum()) + int(d.sum())
+
+
+@pytest.mark.parametrize("leaves", [65535, 65536, 70000])
+def test_c4_counter_width_limits(cuda, leaves):
+    """K_{2,n}: two hubs joined to n leaves hold C(n,2) 4-cycles.  The top hub
+    has n lower neighbours and one wedge end (the other hub) reached n times,
+    so its window counter climbs to n.  Up to 65535 lower neighbours the
+    window kernel packs 16-bit counters (n = 65535 drives one to its maximum);
+    from 65536 it counts 32-bit counters over half windows."""
+    n = leaves + 2
+    a = np.arange(2, n, dtype=np.uint32)
+    src = np.concatenate([np.zeros(leaves, np.uint32), np.ones(leaves, np.uint32)])
+    dst = np.concatenate([a, a])
+    ptr, idx = O.sym_csr(src, dst, n)
+    with gb.Graph.upload(ptr, idx, n) as g:
+        assert g.count(C4) == comb(leaves, 2)
+        assert g.count(K3) == 0
+
+
+def test_c4_many_heavy_hubs(cuda):
+    """Several hubs over a shared leaf set, with leaves also joined in a ring:
+    every pair of hubs closes C(leaves, 2) 4-cycles through two leaves, plus
+    the cycles that use ring edges; the oracle settles the total.  Hubs are
+    heavy vertices whose windows span the whole leaf range."""
+    hubs, leaves = 6, 3000
+    n = hubs + leaves
+    lv = np.arange(hubs, n, dtype=np.uint32)
+    src = np.concatenate([np.full(leaves, h, np.uint32) for h in range(hubs)] + [lv])
+    dst = np.concatenate([lv for _ in range(hubs)] + [np.roll(lv, 1)])
+    ptr, idx = O.sym_csr(src, dst, n)
+    with gb.Graph.upload(ptr, idx, n) as g:
+        assert g.count(C4) == O.c4_count(ptr, idx)
