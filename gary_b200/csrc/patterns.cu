@@ -475,7 +475,7 @@ __global__ void __launch_bounds__(kWinThreads, 3)
 constexpr uint32_t kK4WarpMaxD = 128;         // warp vertices: rows of at most 4 words
 constexpr uint32_t kK4MidMaxD = 512;          // mid vertices: rows of at most 16 words
 constexpr int kK4WarpLog = 8;                 // warp position hash: 256 slots
-constexpr uint32_t kK4WarpWords = 1536;       // shared words per warp
+constexpr uint32_t kK4WarpWords = 1024;       // shared words per warp: 32 KiB per CTA, up to 7 CTAs per SM
 constexpr int kK4WarpCtaWarps = 8;
 constexpr int kK4MidThreads = 256, kK4MidLog = 10;
 constexpr uint32_t kK4MidRowWords = kK4MidMaxD * (kK4MidMaxD / 32);  // 8192
