@@ -78,20 +78,29 @@ __device__ __forceinline__ uint32_t prefix_below(const uint32_t *l, uint32_t len
   return b;
 }
 
+// |N(v) below u| for a lower neighbour v < u: N(v) (ranked, sorted) starts
+// with its deg(v) - d+(v) ids below v, all below u too, so only the d+(v)
+// higher ids need a search (a few probes, not log2 deg(v)).
+__device__ __forceinline__ uint32_t below_u(const uint32_t *l, uint32_t len, uint32_t dplus_v, uint32_t u) {
+  const uint32_t lower = len - dplus_v;
+  return lower + prefix_below(l + lower, dplus_v, u);
+}
+
 // Walk every wedge u - v - w with v in N(u), v < u, and w in N(v), w < u,
 // for v = N(u)[k], k in the 32-wide steps kb, kb + kstep, ... < ke; call
 // f(w) for each.  All 32 lanes must call.
 template <typename F>
-__device__ __forceinline__ void c4_wedges(const GraphView &s, const uint32_t *__restrict__ au,
-                                          uint32_t u, uint32_t kb, uint32_t ke, uint32_t kstep,
-                                          int lane, F f) {
+__device__ __forceinline__ void c4_wedges(const GraphView &s, const uint32_t *__restrict__ dplus,
+                                          const uint32_t *__restrict__ au, uint32_t u, uint32_t kb,
+                                          uint32_t ke, uint32_t kstep, int lane, F f) {
   for (uint32_t k0 = kb; k0 < ke; k0 += kstep) {
     const uint32_t k = k0 + lane;
     uint32_t len = 0, base = 0;
     if (k < ke) {
-      const uint2 rv = s.row[au[k]];
+      const uint32_t v = au[k];
+      const uint2 rv = s.row[v];
       base = rv.x;
-      len = prefix_below(s.adj + (uint64_t)rv.x * 4, rv.y, u);
+      len = below_u(s.adj + (uint64_t)rv.x * 4, rv.y, dplus[v], u);
     }
     const uint32_t incl = warp_inclusive_sum(len, lane);
     const uint32_t excl = incl - len;
@@ -146,7 +155,7 @@ __global__ void __launch_bounds__(kPWarps * 32)
         vals[i] = 0;
       }
       __syncwarp();
-      c4_wedges(s, au, u, 0, pre, 32, lane, [&](uint32_t w) {
+      c4_wedges(s, dplus, au, u, 0, pre, 32, lane, [&](uint32_t w) {
         acc += map_incr(keys, vals, kPSlots - 1, 32 - 10, w);
       });
       __syncwarp();
@@ -157,23 +166,45 @@ __global__ void __launch_bounds__(kPWarps * 32)
 }
 
 // ---- C4, medium vertices: one CTA-wide shared hash map per vertex ---------
-constexpr uint32_t kMidSlots = 16384;  // keys + counts: 128 KiB of shared memory
+// A count c(u,w) never exceeds the vertex's wedge count (each v adds at most
+// one to it), at most kMidWedges here, so counts are 16 bits, two to a word:
+// keys 64 KiB + counts 32 KiB, and two CTAs share an SM.
+constexpr uint32_t kMidSlots = 16384;
 constexpr int kMidLog = 14;
 constexpr int kMidThreads = 512;
 constexpr uint64_t kMidWedges = kMidSlots / 2;  // wedges (>= distinct w) a medium vertex may have
+constexpr uint32_t kMidWords = kMidSlots + kMidSlots / 2;
+static_assert(kMidWedges < 65536, "16-bit medium counts");
 
-__global__ void __launch_bounds__(kMidThreads, 1)
+// As map_incr, with the count of slot h in half h & 1 of word h / 2 of vals2.
+__device__ __forceinline__ uint32_t map_incr16(uint32_t *keys, uint32_t *vals2, uint32_t mask, int shift,
+                                               uint32_t w) {
+  uint32_t h = (w * kHashMul) >> shift;
+  while (true) {
+    const uint32_t k = keys[h];
+    bool hit = k == w;
+    if (!hit && k == kSentinel) {
+      const uint32_t old = atomicCAS(&keys[h], kSentinel, w);
+      hit = old == kSentinel || old == w;
+    }
+    if (hit) {
+      const uint32_t sh = (h & 1u) << 4;
+      return (atomicAdd(&vals2[h >> 1], 1u << sh) >> sh) & 0xFFFFu;
+    }
+    h = (h + 1) & mask;
+  }
+}
+
+__global__ void __launch_bounds__(kMidThreads, 2)
     k_c4_mid(GraphView s, const uint32_t *__restrict__ dplus, const uint32_t *__restrict__ mid,
              uint32_t n_mid, SchedState *sched, unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t sm[];
-  uint32_t *keys = sm, *vals = sm + kMidSlots;
+  uint32_t *keys = sm, *vals = sm + kMidSlots;  // vals: kMidSlots / 2 words of 16-bit pairs
   __shared__ uint32_t s_u, s_next;
   const int lane = threadIdx.x & 31;
   unsigned long long acc = 0;
-  for (uint32_t i = threadIdx.x; i < kMidSlots; i += blockDim.x) {
-    keys[i] = kSentinel;
-    vals[i] = 0;
-  }
+  for (uint32_t i = threadIdx.x; i < kMidSlots; i += blockDim.x) keys[i] = kSentinel;
+  for (uint32_t i = threadIdx.x; i < kMidSlots / 2; i += blockDim.x) vals[i] = 0;
   while (true) {
     if (threadIdx.x == 0) {
       s_u = atomicAdd(&sched->next_aux, 1u);
@@ -190,15 +221,13 @@ __global__ void __launch_bounds__(kMidThreads, 1)
       if (lane == 0) k = atomicAdd(&s_next, 32u);
       k = __shfl_sync(kFull, k, 0);
       if (k >= pre) break;
-      c4_wedges(s, au, u, k, min(k + 32, pre), 32, lane, [&](uint32_t w) {
-        acc += map_incr(keys, vals, kMidSlots - 1, 32 - kMidLog, w);
+      c4_wedges(s, dplus, au, u, k, min(k + 32, pre), 32, lane, [&](uint32_t w) {
+        acc += map_incr16(keys, vals, kMidSlots - 1, 32 - kMidLog, w);
       });
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < kMidSlots; i += blockDim.x) {
-      keys[i] = kSentinel;
-      vals[i] = 0;
-    }
+    for (uint32_t i = threadIdx.x; i < kMidSlots; i += blockDim.x) keys[i] = kSentinel;
+    for (uint32_t i = threadIdx.x; i < kMidSlots / 2; i += blockDim.x) vals[i] = 0;
     // the loop head's barrier orders this reset before the next vertex
   }
   acc = warp_sum_u64(acc);
@@ -665,8 +694,9 @@ __global__ void k_c4_exact_wedges(const uint2 *__restrict__ srow, const uint32_t
     const uint32_t pre = ru.y - dplus[u];
     uint64_t w = 0;
     for (uint32_t k = lane; k < pre; k += 32) {
-      const uint2 rv = srow[sadj[(uint64_t)ru.x * 4 + k]];
-      w += prefix_below(sadj + (uint64_t)rv.x * 4, rv.y, u);
+      const uint32_t v = sadj[(uint64_t)ru.x * 4 + k];
+      const uint2 rv = srow[v];
+      w += below_u(sadj + (uint64_t)rv.x * 4, rv.y, dplus[v], u);
     }
     w = warp_sum_u64(w);
     if (lane == 0) wed[i] = w;
@@ -946,7 +976,7 @@ int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   const uint32_t m0 = part(plan->n_mid, shard), m1 = part(plan->n_mid, shard + 1);
   const uint32_t l0 = part(plan->n_light, shard), l1 = part(plan->n_light, shard + 1);
   const size_t smem_small = (size_t)kPWarps * 2 * kPSlots * 4;
-  const size_t smem_mid = (size_t)2 * kMidSlots * 4;
+  const size_t smem_mid = (size_t)kMidWords * 4;
   const size_t smem_win = (size_t)kWinWords * 4;
   static bool attr[64] = {false};
   const int dev = device_ordinal();
@@ -959,6 +989,9 @@ int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   int per_sm = 0;
   GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_c4_small, kPWarps * 32, smem_small));
   if (per_sm < 1) per_sm = 1;
+  int per_sm_mid = 0;
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_mid, k_c4_mid, kMidThreads, smem_mid));
+  if (per_sm_mid < 1) per_sm_mid = 1;
   const GraphView sv{g->n, g->sym.row.p, g->sym.adj.p, true};
   GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
   GARY_CUDA(cudaMemsetAsync(d_out, 0, 8, s));
@@ -967,7 +1000,7 @@ int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
     k_c4_win<<<std::min<uint32_t>(plan->win_ctas, t1 - t0), kWinThreads, smem_win, s>>>(
         sv, plan->tiles.p, t0, t1, plan->cursors.p, std::max(plan->max_pre, 1u), plan->sched.p, d_out);
   if (m1 > m0)
-    k_c4_mid<<<std::min<uint32_t>((uint32_t)sm_count(), m1 - m0), kMidThreads, smem_mid, s>>>(
+    k_c4_mid<<<std::min<uint32_t>((uint32_t)(sm_count() * per_sm_mid), m1 - m0), kMidThreads, smem_mid, s>>>(
         sv, g->dag.outdeg.p, plan->mid.p + m0, m1 - m0, plan->sched.p, d_out);
   if (l1 > l0)
     k_c4_small<<<(unsigned)(sm_count() * per_sm), kPWarps * 32, smem_small, s>>>(
