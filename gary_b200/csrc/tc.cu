@@ -67,6 +67,9 @@ struct MinU64 {
 };
 
 // One candidate per padded word w of N+(u): the suffix after v = adj[w].
+// Words without a record get the key n - 1: in rank ids the top vertex has
+// no higher neighbour, so no record ever targets it, and the keys of an
+// n = 2^k graph fit k bits (one radix pass fewer than with the key n).
 __global__ void k_in_candidates(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
                                 const uint32_t *__restrict__ rowid, uint64_t words, uint32_t n,
                                 uint32_t *__restrict__ keys, uint2 *__restrict__ vals) {
@@ -75,7 +78,7 @@ __global__ void k_in_candidates(const uint2 *__restrict__ row, const uint32_t *_
     const uint32_t u = rowid[w];
     const uint2 r = row[u];
     const uint64_t pos = w - (uint64_t)r.x * 4;
-    uint32_t key = n;
+    uint32_t key = n - 1;
     uint2 val = make_uint2(0, 0);
     if (pos < r.y) {
       const uint32_t v = adj[w];
@@ -325,7 +328,7 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
     cub::DoubleBuffer<uint32_t> kb(keys.p, keys2.p);
     cub::DoubleBuffer<uint2> vb(vals.p, vals2.p);
     size_t tmp = 0;
-    const int eb = bits_for((uint64_t)n + 1);
+    const int eb = bits_for((uint64_t)n);  // keys <= n - 1
     GARY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kb, vb, W, 0, eb, s));
     DevBuf<uint8_t> t;
     GARY_TRY(t.alloc(tmp, s));
@@ -335,12 +338,12 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
   }
   keys2.release();
   vals2.release();
-  // records = number of keys < n (the rest carry the "no record" key n)
+  // records = number of keys < n - 1 (the rest carry the "no record" key n - 1)
   uint64_t m = 0;
   {
     DevBuf<uint64_t> pos;
     GARY_TRY(pos.alloc(1, s));
-    k_first_geq<<<1, 1, 0, s>>>(keys.p, W, n, pos.p);
+    k_first_geq<<<1, 1, 0, s>>>(keys.p, W, n - 1, pos.p);
     GARY_CUDA(cudaGetLastError());
     GARY_CUDA(cudaMemcpyAsync(&m, pos.p, 8, cudaMemcpyDeviceToHost, s));
     GARY_CUDA(cudaStreamSynchronize(s));
