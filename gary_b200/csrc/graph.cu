@@ -164,46 +164,48 @@ __device__ __forceinline__ bool kept_entry(uint32_t a, uint32_t b, const uint32_
   return true;
 }
 
+// Per input entry e: its ranked row r = rank[s] and target rank[t], and its
+// slot in row r (the old value of the row's count), so that the fill is a
+// streaming pass.  Entries that are not kept get ent[e].x = kSentinel.
 __global__ void k_count_rows(const uint32_t *__restrict__ rowid, const uint32_t *__restrict__ idx,
                              uint64_t nnz, uint32_t n, const uint32_t *__restrict__ deg,
                              const uint32_t *__restrict__ rank, bool dag, bool validate,
                              uint32_t *__restrict__ dplus, unsigned long long *__restrict__ kept,
-                             unsigned *err) {
+                             unsigned *err, uint2 *__restrict__ ent, uint32_t *__restrict__ eslot) {
   unsigned long long mine = 0;
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < nnz;
        e += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t a = rowid[e], b = idx[e];
+    uint2 en = make_uint2(kSentinel, 0u);
+    uint32_t slot = 0;
+    uint32_t su, tv;
     if (b >= n) {
       atomicOr(err, kErrRange);
-      continue;
-    }
-    if (a == b) {
+    } else if (a == b) {
       atomicOr(err, kErrLoop);
-      continue;
+    } else {
+      if (validate && e + 1 < nnz && rowid[e + 1] == a && idx[e + 1] <= b) atomicOr(err, kErrOrder);
+      if (kept_entry(a, b, deg, dag, su, tv)) {
+        en.x = rank[su];
+        en.y = rank[tv];
+        slot = atomicAdd(&dplus[en.x], 1u);
+        ++mine;
+      }
     }
-    if (validate && e + 1 < nnz && rowid[e + 1] == a && idx[e + 1] <= b) atomicOr(err, kErrOrder);
-    uint32_t su, tv;
-    if (!kept_entry(a, b, deg, dag, su, tv)) continue;
-    atomicAdd(&dplus[rank[su]], 1u);
-    ++mine;
+    ent[e] = en;
+    eslot[e] = slot;
   }
   for (int o = 16; o; o >>= 1) mine += __shfl_xor_sync(kFull, mine, o);
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(kept, mine);
 }
 
-__global__ void k_fill_rows(const uint32_t *__restrict__ rowid, const uint32_t *__restrict__ idx,
-                            uint64_t nnz, uint32_t n, const uint32_t *__restrict__ deg,
-                            const uint32_t *__restrict__ rank, bool dag, const uint2 *__restrict__ row,
-                            uint32_t *__restrict__ cursor, uint32_t *__restrict__ adj) {
+__global__ void k_fill_rows(const uint2 *__restrict__ ent, const uint32_t *__restrict__ eslot, uint64_t nnz,
+                            const uint2 *__restrict__ row, uint32_t *__restrict__ adj) {
   for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < nnz;
        e += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t a = rowid[e], b = idx[e];
-    if (b >= n || a == b) continue;
-    uint32_t su, tv;
-    if (!kept_entry(a, b, deg, dag, su, tv)) continue;
-    const uint32_t r = rank[su];
-    const uint32_t slot = atomicAdd(&cursor[r], 1u);
-    adj[(uint64_t)row[r].x * 4 + slot] = rank[tv];
+    const uint2 en = ent[e];
+    if (en.x == kSentinel) continue;
+    adj[(uint64_t)row[en.x].x * 4 + eslot[e]] = en.y;
   }
 }
 
@@ -678,9 +680,13 @@ int ranked_dag_by_rows(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz
   DevBuf<unsigned long long> dkept;
   GARY_TRY(dkept.alloc(1, s));
   GARY_CUDA(cudaMemsetAsync(dkept.p, 0, 8, s));
+  DevBuf<uint2> ent;      // per entry: ranked row, target rank
+  DevBuf<uint32_t> eslot; // per entry: slot in its row
+  GARY_TRY(ent.alloc(std::max<uint64_t>(nnz, 1), s));
+  GARY_TRY(eslot.alloc(std::max<uint64_t>(nnz, 1), s));
   if (nnz)
     k_count_rows<<<grid_for(nnz), kThreads, 0, s>>>(rowid, didx, nnz, n, deg, rank, dag, validate,
-                                                    c.outdeg.p, dkept.p, err);
+                                                    c.outdeg.p, dkept.p, err, ent.p, eslot.p);
   GARY_CUDA(cudaGetLastError());
   DevBuf<uint64_t> off4;
   GARY_TRY(off4.alloc((uint64_t)n + 1, s));
@@ -712,15 +718,10 @@ int ranked_dag_by_rows(const uint32_t *rowid, const uint32_t *didx, uint64_t nnz
   GARY_CUDA(cudaGetLastError());
   off4.release();
   tr.mark("allocate + records");
-  {
-    DevBuf<uint32_t> cursor;
-    GARY_TRY(cursor.alloc(n, s));
-    GARY_CUDA(cudaMemsetAsync(cursor.p, 0, (uint64_t)n * 4, s));
-    if (nnz)
-      k_fill_rows<<<grid_for(nnz), kThreads, 0, s>>>(rowid, didx, nnz, n, deg, rank, dag, c.row.p,
-                                                     cursor.p, c.adj.p);
-    GARY_CUDA(cudaGetLastError());
-  }
+  if (nnz) k_fill_rows<<<grid_for(nnz), kThreads, 0, s>>>(ent.p, eslot.p, nnz, c.row.p, c.adj.p);
+  GARY_CUDA(cudaGetLastError());
+  ent.release();
+  eslot.release();
   tr.mark("fill");
   // order every row in place
   if (m) {
