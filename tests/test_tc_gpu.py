@@ -296,3 +296,27 @@ def test_complete_graph_long_rows(cuda, k):
         assert np.all(np.diff(dp.astype(np.int64)) == np.arange(k - 1, -1, -1))
         want = np.concatenate([np.arange(u + 1, k, dtype=np.uint32) for u in range(k)])
         assert np.array_equal(di, want)
+
+
+def test_block_cache_reuse_across_shapes(cuda):
+    """Freed graphs hand their device blocks to later uploads (the library's
+    block cache): graphs of three sizes, uploaded, freed out of order and
+    uploaded again, keep their exact counts."""
+    cases = []
+    for scale, ef, seed in ((12, 8, 1), (15, 16, 2), (13, 4, 3)):
+        n = 1 << scale
+        src, dst = gb.gen_rmat(scale, seed, ef << scale)
+        ptr, idx = gb.csr_from_edges(src, dst, n)
+        optr, oidx = O.orient(ptr, idx)
+        cases.append((ptr, idx, n, O.tri_count(optr, oidx)))
+    live = [_upload_host(p, i, n) for p, i, n, _ in cases]
+    for g, (_, _, _, want) in zip(live, cases):
+        assert g.count() == want
+    live[1].free()
+    live[0].free()
+    again = [_upload_host(p, i, n) for p, i, n, _ in reversed(cases)]
+    for g, (_, _, _, want) in zip(again, reversed(cases)):
+        assert g.count() == want
+    live[2].free()
+    for g in again:
+        g.free()
