@@ -277,8 +277,12 @@ __device__ __forceinline__ uint32_t gallop_geq(const uint32_t *l, uint32_t c, ui
 // with kSentinel to a multiple of 8): the 16 ids of the two octets from c's
 // octet come in one round of loads and settle most runs (70 % of a window's
 // runs hold at most 8 ids); only a run that goes past them gallops on.
-__device__ __forceinline__ uint32_t run_end(const uint32_t *l, uint32_t c, uint32_t len, uint32_t x) {
-  if (c >= len) return c;
+__device__ __forceinline__ uint32_t run_end(const uint32_t *l, uint32_t c, uint32_t len, uint32_t x,
+                                            uint32_t *at_end = nullptr) {
+  if (c >= len) {
+    if (at_end) *at_end = kSentinel;
+    return c;
+  }
   const uint32_t ob = c & ~7u;
   const uint32_t plen = (len + 7u) & ~7u;
   const uint4 *q = reinterpret_cast<const uint4 *>(l + ob);
@@ -288,12 +292,19 @@ __device__ __forceinline__ uint32_t run_end(const uint32_t *l, uint32_t c, uint3
   const uint4 b0 = two ? q[2] : s4, b1 = two ? q[3] : s4;
   const uint32_t id[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
                            b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-  uint32_t e = kSentinel;
+  uint32_t e = kSentinel, ide = kSentinel;
 #pragma unroll
   for (int i = 15; i >= 0; --i)
-    if (ob + i >= c && (ob + i >= len || id[i] >= x)) e = ob + i;
-  if (e != kSentinel) return e;
-  return gallop_geq(l, ob + 16, len, x);  // ids [c, ob + 16) are all below x
+    if (ob + i >= c && (ob + i >= len || id[i] >= x)) {
+      e = ob + i;
+      ide = ob + i < len ? id[i] : kSentinel;
+    }
+  if (e == kSentinel) {
+    e = gallop_geq(l, ob + 16, len, x);  // ids [c, ob + 16) are all below x
+    ide = e < len ? l[e] : kSentinel;
+  }
+  if (at_end) *at_end = ide;  // the id at e (kSentinel at the end of the list)
+  return e;
 }
 
 __device__ __forceinline__ uint32_t warp_min_u32(uint32_t x) {
@@ -392,7 +403,7 @@ __global__ void __launch_bounds__(kWinThreads, 3)
     for (uint32_t k = threadIdx.x; k < pre; k += blockDim.x) {
       const uint2 rv = s.row[au[k]];
       const uint32_t *l = s.adj + (uint64_t)rv.x * 4;
-      const uint32_t c = lower_bound_u32(l, 0, rv.y, w_begin);
+      const uint32_t c = w_begin ? lower_bound_u32(l, 0, rv.y, w_begin) : 0u;
       const uint32_t x = c < rv.y ? l[c] : kSentinel;
       const uint32_t nw = x < w_end ? x / ws : kNoWindow;
       cs.vrow[k] = rv;
@@ -448,10 +459,10 @@ __global__ void __launch_bounds__(kWinThreads, 3)
           const uint2 rv = cs.vrow[k];
           const uint32_t *l = s.adj + (uint64_t)rv.x * 4;
           b = cs.cur[k];
-          e = run_end(l, b, rv.y, hi);
+          uint32_t x;
+          e = run_end(l, b, rv.y, hi, &x);
           cs.prev[k] = b;
           cs.cur[k] = e;
-          const uint32_t x = e < rv.y ? l[e] : kSentinel;
           const uint32_t nw = x < w_end ? x / ws : kNoWindow;
           cs.nextw[k] = nw;
           nxt = min(nxt, nw);
