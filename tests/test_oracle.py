@@ -79,6 +79,20 @@ def test_small_kats():
     assert counts(5, [(0, 2), (0, 3), (0, 4), (1, 2), (1, 3), (1, 4)]) == (0, 3, 0)
 
 
+@pytest.mark.parametrize("leaves", [1000, 65535, 70000])
+def test_two_hub_bipartite_c4(leaves):
+    """K_{2,n} holds C(n,2) 4-cycles and nothing else; the GPU tests use the
+    same graphs at the window kernel's counter-width limits."""
+    n = leaves + 2
+    a = np.arange(2, n, dtype=np.uint32)
+    src = np.concatenate([np.zeros(leaves, np.uint32), np.ones(leaves, np.uint32)])
+    dst = np.concatenate([a, a])
+    ptr, idx = O.sym_csr(src, dst, n)
+    dptr, didx = O.orient(ptr, idx)
+    assert O.c4_count(ptr, idx) == comb(leaves, 2)
+    assert O.tri_count(dptr, didx) == 0 and O.k4_count(dptr, didx) == 0
+
+
 def test_c4_trace_identity(golden):
     """tr(A^4) = 8 C4 + 2 sum d(d-1) + 2m on real fixtures: two independent
     computations of the 4-cycle count agree."""
