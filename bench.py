@@ -9,6 +9,9 @@ Multi-GPU (torchrun, one rank per GPU): every rank holds the whole graph and
 counts its shard of the tile plan; the shard counts are summed with one 8-byte
 all-reduce (strong scaling).
 
+`learned` times the same count under the learned schedule (the cost model in
+gary_b200/data) right after the plain one, in the same process.
+
 `e2e` runs the same count through the public C ABI from pinned HOST buffers:
 upload (H2D copy, orientation, relabel, padding) + count + the 8-byte D2H read
 of the result, every step.  The host graph is the reference's input form for
@@ -16,9 +19,16 @@ this path by default: the id-oriented DAG CSR (csr_dag.bin, each edge once in
 the row of its larger endpoint); --e2e-input symmetric uploads both directions.
 
 `cpu_baseline` (rank 0, N=1) and `--impl reference` time the reference's own CPU
-implementation (cpuTriCount over the reference's GraphCSR, compiled in place
-under oracle/_ref) on a bounded, evenly strided sample of the same graph's
-vertices, with all host threads.
+path: the same seeded edges (the oracle's restatement of the generator, so the
+product library is not loaded), deduplicated, then the reference's own graph
+pipeline (GraphCOO::symmetrize -> toCSR_ -> toCOO -> orientation -> toCSR_,
+src/Graph.cpp, compiled in place under oracle/_ref) and its cpuTriCount
+(test/TriQueryTest.cu:17-37) on a bounded, evenly strided vertex sample, with
+all host threads.
+
+`batch` and `setops` (N=1; --no-extras skips them) summarise the batched
+4096-graph launch and the set-intersection microbench on a 2^20-pair batch;
+`--workload batch|setops|patterns` runs each in full.
 """
 from __future__ import annotations
 
@@ -68,6 +78,9 @@ def parse():
     ap.add_argument("--pairs-log2", type=int, default=24, help="setops: total pairs = 2^k")
     ap.add_argument("--batch-log2", type=int, default=20, help="setops: pairs per generated batch")
     ap.add_argument("--overlaps", default="0,0.1,0.25,0.5", help="setops: planted overlap fractions")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-schedule leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batch and set-intersection summaries of the default line")
     return ap.parse_args()
 
 
@@ -165,64 +178,116 @@ def id_oriented_dag(torch, hp, hi, n):
     return op, oi, nnz
 
 
-def traffic_per_launch(workload: str):
+def workload_config(args, world: int) -> dict:
+    """The `config` both arms print (the same dict, so the lines compare)."""
+    return {"workload": f"triangle count, RMAT scale {args.scale} edge factor {args.ef}, seed {args.seed}",
+            "scale": args.scale, "ef": args.ef, "seed": args.seed,
+            "l2": "inputs larger than L2: the graph's lists (GBs) against the 126 MB L2",
+            "parallelism": f"dp{world} (tile shards, graph replicated)"}
+
+
+# Sources the triangle kernel is built from: a counter capture stored under
+# profiles/ applies to the build whose sources hash to its "kernel_src".
+KERNEL_SOURCES = ("tc.cu", "tc.cuh", "warp_ops.cuh", "bulk.cuh", "internal.cuh", "graph.cuh")
+
+
+def kernel_source_hash() -> str:
+    import hashlib
+
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        h.update((ROOT / "gary_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()[:16]
+
+
+def measured_counters(workload: str):
+    """The ncu counters stored for `workload` (profiles/roofline_traffic.json:
+    DRAM bytes, warp instructions and L2->SM bytes of one launch), with
+    `stale` true when they were captured on other kernel sources."""
     f = ROOT / "profiles" / "roofline_traffic.json"
     if not f.exists():
         return None
     try:
-        d = json.loads(f.read_text())
-        return d.get(workload)
+        rec = json.loads(f.read_text()).get(workload)
     except Exception:
         return None
+    if not isinstance(rec, dict):
+        return None
+    rec = dict(rec)
+    rec["stale"] = rec.get("kernel_src") != kernel_source_hash()
+    return rec
 
 
-def cpu_reference_sample(O, dag_ptr, dag_idx, target_s: float):
-    """Time the reference's cpuTriCount on an evenly strided vertex sample."""
+def peak_hbm():
+    pk = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(pk.read_text()) if pk.exists() else {}
+    hbm = peaks.get("hbm_gbs")
+    if hbm:
+        return float(hbm), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    return 6650.0, "fallback 6650 GB/s"
+
+
+def reference_dag(scale: int, ef: int, seed: int):
+    """The reference's oriented CSR of the workload, built without the product
+    library: the oracle's restatement of the seeded generator, the duplicate
+    and loop removal the workload defines, then the reference's own pipeline
+    (symmetrize -> toCSR_ -> toCOO -> orientation -> toCSR_, src/Graph.cpp; the
+    orientation keeps src > dst, as convert.cpp writes csr_dag.bin).
+    Returns (RefCSR, out-degrees, oriented edges, seconds)."""
     import numpy as np
 
-    n = len(dag_ptr) - 1
-    ref = O.RefCSR.from_arrays(dag_ptr.astype(np.int64), dag_idx.astype(np.int32))
-    threads = O.ref_cpu().ref_omp_max_threads()
-    deg = np.diff(dag_ptr.astype(np.int64))
+    from oracle import oracle as O
 
-    def run(stride):
+    n = 1 << scale
+    t0 = time.perf_counter()
+    src, dst = O.gen_rmat(scale, seed, ef << scale)
+    us, vs = O.unique_edges(n, src, dst)
+    del src, dst
+    ref = O.RefCSR.dag_from_edges(n, us.view(np.int32), vs.view(np.int32))
+    m = len(us)
+    del us, vs
+    ptr, _ = ref.arrays()
+    deg = np.diff(ptr)
+    return ref, deg, m, time.perf_counter() - t0
+
+
+def reference_stride(ref, deg, n: int, target_s: float) -> int:
+    """Vertex stride whose strided sample takes about target_s seconds."""
+    stride = 4096
+    while True:
         edges = int(deg[::stride].sum())
         t0 = time.perf_counter()
         ref.tri_count(0, n, stride, 0)
-        return edges, time.perf_counter() - t0
-
-    stride = 4096
-    edges, dt = run(stride)
-    while dt < 0.5 and stride > 1:
+        dt = time.perf_counter() - t0
+        if dt >= 0.5 or stride == 1:
+            break
         stride = max(1, stride // 8)
-        edges, dt = run(stride)
     rate = edges / max(dt, 1e-9)
-    total_edges = int(deg.sum())
-    want_edges = rate * target_s
-    stride = max(1, int(total_edges / max(want_edges, 1)))
-    return ref, threads, stride, deg
+    return max(1, int(int(deg.sum()) / max(rate * target_s, 1)))
+
+
+def reference_sample_line(ref, deg, m: int, n: int, stride: int, times: list, threads: int, prep_s: float):
+    edges = int(deg[::stride].sum())
+    dt = sum(times) / len(times)
+    sample = (f"every {stride}-th vertex of the reference's id-oriented DAG of the same graph (~{edges} of {m} "
+              f"oriented edges per step, offset rotated per step; input built by the reference's own "
+              f"pipeline in {prep_s:.0f} s, untimed)")
+    return edges / dt, dt, sample
 
 
 # ---------------------------------------------------------------- arms
 def run_reference(args, dist):
-    """--impl reference: the reference's CPU path, rank 0 only."""
-    import numpy as np
-    import torch
-
-    import gary_b200 as gb
+    """--impl reference: the reference's CPU path, rank 0 only.  Nothing of the
+    product library is loaded: the input comes from the oracle's generator
+    restatement and the reference's own pipeline."""
     from oracle import oracle as O
 
     if dist.rank != 0:
         return 0
-    torch.cuda.set_device(dist.local)
-    n, csr = build_graph(gb, torch, args.scale, args.ef, args.seed)
-    g = upload_from_device_csr(gb, csr, n)
-    csr.free()
-    dptr, didx, _ = g.download()
-    m = len(didx)
-    g.free()
-    ref, threads, stride, deg = cpu_reference_sample(O, dptr, didx, args.cpu_seconds / 2)
-    edges = int(deg[::stride].sum())
+    n = 1 << args.scale
+    ref, deg, m, prep_s = reference_dag(args.scale, args.ef, args.seed)
+    threads = O.ref_cpu().ref_omp_max_threads()
+    stride = reference_stride(ref, deg, n, args.cpu_seconds / 2)
     for _ in range(args.warmup):
         ref.tri_count(0, n, stride * 4, 0)
     times = []
@@ -230,24 +295,64 @@ def run_reference(args, dist):
         t0 = time.perf_counter()
         ref.tri_count(k % stride, n, stride, 0)
         times.append(time.perf_counter() - t0)
-    dt = sum(times) / len(times)
-    value = edges / dt
-    sample = (f"every {stride}-th vertex of the degree-oriented RMAT-{args.scale} ef{args.ef} DAG "
-              f"(~{edges} of {m} oriented edges per step, offset rotated per step)")
+    value, dt, sample = reference_sample_line(ref, deg, m, n, stride, times, threads, prep_s)
+    ref.free()
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"triangle count, RMAT scale {args.scale} edge factor {args.ef}, seed {args.seed}",
-                   "scale": args.scale, "ef": args.ef, "seed": args.seed},
+        "config": workload_config(args, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "path": "cpuTriCount (test/TriQueryTest.cu:17-37, uint64 accumulators) over the reference's GraphCSR",
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def time_counts(L, g, sched, dist, stream, out, steps: int, warmup: int, clocks=None):
+    """Per-step kernel ms (CUDA events on the counting stream) of `steps`
+    counts after `warmup`, bracketed by barriers and synchronisations; then
+    the launch status is checked.  Returns (ms list, local count)."""
+    import ctypes as C
+
+    import torch
+
+    from gary_b200 import _lib
+
+    def step():
+        _lib.check(L.gary_count_shard_async(g.handle, _lib.GARY_PATTERN_TRIANGLE, sched, dist.rank, dist.world,
+                                            C.c_void_p(stream.cuda_stream), C.c_void_p(out.data_ptr())),
+                   "gary_count_shard_async")
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(warmup, 1)):
+            step()
+    stream.synchronize()
+    count_local = int(out.item())
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    dist.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            evs[k][0].record(stream)
+            step()
+            evs[k][1].record(stream)
+    stream.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
+    # the launches' own status (bounded waits, table capacity): never a silent count
+    _lib.check(L.gary_count_status(g.handle, C.c_void_p(stream.cuda_stream)), "gary_count_status")
+    assert int(out.item()) == count_local, "count changed between steps"
+    return [a.elapsed_time(b) for a, b in evs], count_local, clk
+
+
 def run_ours(args, dist):
+    import ctypes as C
+
     import numpy as np
     import torch
 
@@ -259,6 +364,10 @@ def run_ours(args, dist):
     if args.pool_keep_gb is not None:
         _lib.check(_lib.load().gary_tune(b"pool_keep_bytes", int(args.pool_keep_gb * 1e9)), "gary_tune")
     sched = {"plain": _lib.GARY_SCHED_PLAIN, "learned": _lib.GARY_SCHED_LEARNED}[args.sched]
+    if args.sched == "learned" or not args.no_learned:
+        from gary_b200.costmodel import CostModel
+
+        CostModel.load().install()
     t_build = time.perf_counter()
     n, csr = build_graph(gb, torch, args.scale, args.ef, args.seed)
     _, sym_nnz = csr.shape()
@@ -270,37 +379,26 @@ def run_ours(args, dist):
     out = torch.zeros(1, dtype=torch.int64, device="cuda")
     L = _lib.load()
 
-    def step():
-        _lib.check(L.gary_count_shard_async(g.handle, _lib.GARY_PATTERN_TRIANGLE, sched, dist.rank,
-                                            dist.world, C.c_void_p(stream.cuda_stream),
-                                            C.c_void_p(out.data_ptr())), "gary_count_shard_async")
-
-    with torch.cuda.stream(stream):
-        for _ in range(max(args.warmup, 1)):
-            step()
-    stream.synchronize()
-    count_local = int(out.item())
-
     # ---- timed region: K steps, device events on the launching stream
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    clocks = Clocks(dev)
-    dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            evs[k][0].record(stream)
-            step()
-            evs[k][1].record(stream)
-    stream.synchronize()
-    dist.barrier()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    per = [a.elapsed_time(b) for a, b in evs]
+    per, count_local, clk = time_counts(L, g, sched, dist, stream, out, args.steps, args.warmup, Clocks(dev))
+    stats = g.last_stats()
     ms_local = sum(per) / len(per)
     ms = dist.allreduce(ms_local, "max")
     count = dist.allreduce(count_local, "sum")
     value = m / (ms / 1e3)
+
+    # ---- the other schedule on the same graph, same process, same timing rules
+    learned = None
+    if not args.no_learned:
+        other = _lib.GARY_SCHED_PLAIN if args.sched == "learned" else _lib.GARY_SCHED_LEARNED
+        lper, lcount, _ = time_counts(L, g, other, dist, stream, out, args.steps, args.warmup)
+        lms = dist.allreduce(sum(lper) / len(lper), "max")
+        lcount = dist.allreduce(lcount, "sum")
+        learned_ms, plain_ms = (lms, ms) if other == _lib.GARY_SCHED_LEARNED else (ms, lms)
+        learned = {"value": m / (learned_ms / 1e3), "unit": UNIT, "ms": learned_ms, "plain_ms": plain_ms,
+                   "ratio_vs_plain": plain_ms / learned_ms, "count_equal": lcount == count,
+                   "model": "gary_b200/data/cost_model.gmlp (6-64-64-4 MLP, per-vertex variant and tile weights)"}
+        assert lcount == count, f"learned schedule count {lcount} != plain {count}"
 
     # ---- end to end through the public API from pinned host memory
     e2e = None
@@ -317,7 +415,6 @@ def run_ours(args, dist):
             # src > dst, so row u lists its neighbours v < u), built here, untimed
             hp, hi, e2e_nnz = id_oriented_dag(torch, hp, hi, n)
             e2e_flags = _lib.GARY_INPUT_DAG
-        res = C.c_uint64()
         e2e_times = []
         for k in range(args.e2e_steps + 1):
             dist.barrier()
@@ -333,12 +430,13 @@ def run_ours(args, dist):
             with torch.cuda.stream(stream):  # 8-byte D2H read of the result, on the counting stream
                 hres = dres.to("cpu", non_blocking=True)
             stream.synchronize()
-            res.value = int(hres.item())
+            res = int(hres.item())
             dt = time.perf_counter() - t0
+            _lib.check(L.gary_count_status(gh, C.c_void_p(stream.cuda_stream)), "gary_count_status")
             L.gary_graph_free(gh)
             if k > 0:  # first one warms the allocator
                 e2e_times.append(dt)
-            assert res.value == count_local, "e2e count differs from the resident-graph count"
+            assert res == count_local, "e2e count differs from the resident-graph count"
         # the median step, with the mean and every step beside it: a rare step pays
         # for a slow driver call on a host shared with other jobs
         e2e_s = dist.allreduce(statistics.median(e2e_times), "max")
@@ -354,55 +452,64 @@ def run_ours(args, dist):
 
     line = None
     if dist.rank == 0:
-        workload = f"triangle count, RMAT scale {args.scale} edge factor {args.ef}, seed {args.seed}"
+        cfg = workload_config(args, dist.world)
         alg = info["alg_bytes"]
-        from json import loads
-        peaks = {}
-        pk = ROOT / "MEASURED_PEAKS.json"
-        if pk.exists():
-            peaks = loads(pk.read_text())
-        hbm = peaks.get("hbm_gbs")
-        peak_src = "MEASURED_PEAKS.json hbm_gbs (measured)" if hbm else "fallback 6650 GB/s"
-        hbm = hbm or 6650.0
+        hbm, peak_src = peak_hbm()
         # per-launch kernel time at N ranks: each rank runs one launch over its shard
         achieved = (alg / dist.world) / (ms_local / 1e3) / 1e9
-        traffic = traffic_per_launch(workload if dist.world == 1 else "")
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                    "traffic": None, "peak_source": peak_src, "alg_bytes_per_launch": alg / dist.world,
+                    "alg_bytes_definition": "sum over oriented edges of 4(d+(u)+d+(v)) + 24: both lists read "
+                                            "once per edge, as the reference's kernel reads them; the "
+                                            "middle-vertex walk reads far less, so this frac exceeds 1"}
+        mc = measured_counters(cfg["workload"]) if dist.world == 1 else None
+        sm_hz = (clk.get("sm_mhz") or 1965.0) * 1e6 if clk else 1965.0 * 1e6
+        if mc:
+            t = ms_local / 1e3
+            roofline["traffic"] = mc["dram_bytes"]
+            roofline["measured"] = {
+                "source": mc.get("profile"), "kernel_src": mc.get("kernel_src"), "stale": mc["stale"],
+                # DRAM: the bytes one launch moved (ncu) over its live duration
+                "dram": {"gbs": mc["dram_bytes"] / t / 1e9, "frac": mc["dram_bytes"] / t / 1e9 / hbm},
+                # instruction issue: warp instructions (ncu) over 148 SMs x 4 schedulers x clock
+                "issue": {"warp_inst_per_launch": mc.get("warp_inst"),
+                          "ceiling_per_s": sm_count() * 4 * sm_hz,
+                          "frac": (mc["warp_inst"] / t) / (sm_count() * 4 * sm_hz) if mc.get("warp_inst") else None},
+                # L2 -> SM bytes (ncu) and the L2's own throughput fraction (ncu's peak)
+                "l2": {"bytes_to_sm": mc.get("l2_to_sm_bytes"),
+                       "gbs": mc["l2_to_sm_bytes"] / t / 1e9 if mc.get("l2_to_sm_bytes") else None,
+                       "throughput_pct_of_peak": mc.get("l2_pct_of_peak")},
+            }
+        work = stats.get("work") or 0
+        roofline["probes"] = {"per_launch": work, "per_s": work / (ms_local / 1e3) if work else None,
+                              "definition": "ids of in-neighbour suffixes tested against a set of N+(v)"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "sched": args.sched,
-            "config": {
-                "workload": workload, "scale": args.scale, "ef": args.ef, "seed": args.seed, "n": n,
-                "oriented_edges": m, "sym_nnz": sym_nnz, "max_out_degree": info["max_out_degree"],
-                "wedges": info["wedges"], "alg_bytes": alg,
-                "l2": f"inputs larger than L2: adjacency {info['adj_words'] * 4 / 1e9:.2f} GB vs 0.126 GB L2",
-                "parallelism": f"dp{dist.world} (tile shards, graph replicated)",
-            },
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "sched": args.sched,
+            "config": cfg,
+            "graph": {"n": n, "oriented_edges": m, "sym_nnz": sym_nnz, "max_out_degree": info["max_out_degree"],
+                      "wedges": info["wedges"], "alg_bytes": alg, "adj_gb": info["adj_words"] * 4 / 1e9},
             "count": count,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
-                         "alg_bytes_per_launch": alg / dist.world,
-                         # DRAM bytes one launch moved (ncu, same workload) over its live duration:
-                         # the middle-vertex walk serves most list reads from L2, so this sits
-                         # far below the algorithmic figure
-                         "dram_gbs": traffic / (ms_local / 1e3) / 1e9 if traffic else None,
-                         "dram_frac": traffic / (ms_local / 1e3) / 1e9 / hbm if traffic else None},
+            "roofline": roofline,
+            "learned": learned,
             "e2e": e2e,
             "gpu_launches": args.steps,
             "clocks": clk,
             "build_s": build_s,
+            "cta_path_tiles": stats.get("cta_path_tiles"),
         }
     g_dag = None
-    if dist.rank == 0 and dist.world == 1 and (not args.no_cpu or not args.no_ref_gpu):
+    if dist.rank == 0 and dist.world == 1 and not args.no_ref_gpu:
         g_dag = g.download()
     g.free()
+    torch.cuda.empty_cache()
 
-    if dist.rank == 0 and dist.world == 1 and g_dag is not None:
-        from oracle import oracle as O  # CPU baseline / reference leg only
+    if dist.rank == 0 and dist.world == 1:
+        from oracle import oracle as O  # CPU baseline / reference legs only
 
-        dptr, didx, _ = g_dag
-        if not args.no_ref_gpu and O.have_ref_gpu():
+        if g_dag is not None and O.have_ref_gpu():
+            dptr, didx, _ = g_dag
             # the reference's own triangleCountHom<true,32> built for sm_100a, same DAG
             ref = O.RefGpuGraph(dptr.astype(np.int64), didx.astype(np.int32))
             ref.tri_count(0)
@@ -416,24 +523,55 @@ def run_ours(args, dist):
             line["ref_gpu_kernel"] = {"value": m / (tr / 1e3), "unit": UNIT, "ms": tr,
                                       "kernel": "graph_query::triangleCountHom<true,32> (sm_100a build)",
                                       "count_equal": True}
+        del g_dag
         if not args.no_cpu and O.have_ref_cpu():
-            ref, threads, stride, deg = cpu_reference_sample(O, dptr, didx, args.cpu_seconds)
-            edges = int(deg[::stride].sum())
+            ref, deg, rm, prep_s = reference_dag(args.scale, args.ef, args.seed)
+            threads = O.ref_cpu().ref_omp_max_threads()
+            stride = reference_stride(ref, deg, n, args.cpu_seconds)
             t0 = time.perf_counter()
             ref.tri_count(0, n, stride, 0)
             dt = time.perf_counter() - t0
-            line["cpu_baseline"] = {
-                "value": edges / dt, "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": f"every {stride}-th vertex ({edges} oriented edges, {dt:.1f} s) of the same DAG",
-            }
+            v, _, sample = reference_sample_line(ref, deg, rm, n, stride, [dt], threads, prep_s)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                                    "sample": sample}
             ref.free()
+        if not args.no_extras:
+            line["batch"] = batch_summary(args)
+            line["setops"] = setops_summary(args)
     if line is not None:
         print(json.dumps(line), flush=True)
     dist.close()
     return 0
 
 
+def sm_count() -> int:
+    import torch
+
+    return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+
+
 def run_setops(args, dist):
+    import torch
+
+    torch.cuda.set_device(dist.local)
+    overlaps = [float(x) for x in args.overlaps.split(",")]
+    print(json.dumps(setops_measure(args, args.pairs_log2, args.batch_log2, overlaps, not args.no_cpu)), flush=True)
+    return 0
+
+
+def setops_summary(args) -> dict:
+    """The microbench on one 2^20-pair batch at planted overlap 0.1, for the
+    default line: pairs/s per variant (count only), the best variant's HBM
+    fraction, the CPU merge baseline, and whether every variant agreed."""
+    line = setops_measure(args, 20, 20, [0.1], True)
+    per = {k.split(":")[1]: round(r["pairs_per_s"]) for k, r in line["variants"].items() if k.endswith(":count")}
+    return {"metric": "set-intersection pairs/s", "pairs": 1 << 20, "overlap": 0.1, "pairs_per_s": per,
+            "best": line["best"], "best_pairs_per_s": line["value"], "roofline": line["roofline"],
+            "cpu_baseline": line["cpu_baseline"], "variants_agree": True,
+            "full_run": "python bench.py --workload setops (2^24 pairs per overlap, overlaps 0-0.5)"}
+
+
+def setops_measure(args, pairs_log2: int, batch_log2: int, overlaps: list, with_cpu: bool) -> dict:
     """Set-intersection microbench: 2^pairs_log2 pairs of sorted uint32 lists,
     Zipf(1.2) lengths on [1, 65536], values in [0, 2^26), per planted overlap;
     merge / two-phase search / bitmap / auto, count-only and materialised.
@@ -448,11 +586,9 @@ def run_setops(args, dist):
     from gary_b200 import setops as so
     from oracle import oracle as O
 
-    torch.cuda.set_device(dist.local)
     cdf = so.zipf_table(65536, 1.2)
-    total_pairs = 1 << args.pairs_log2
-    bsz = min(1 << args.batch_log2, total_pairs)
-    overlaps = [float(x) for x in args.overlaps.split(",")]
+    total_pairs = 1 << pairs_log2
+    bsz = min(1 << batch_log2, total_pairs)
     variants = ["merge", "search", "bitmap", "auto"]
     res = {}
     stream = torch.cuda.Stream()
@@ -483,7 +619,7 @@ def run_setops(args, dist):
                     launches += 1
                     acc[(v, mat)][0] += e0.elapsed_time(e1)
                     acc[(v, mat)][1] += int(tot.item())
-            if cpu is None and not args.no_cpu:
+            if cpu is None and with_cpu:
                 # CPU merge on a sample of this batch, checked against the GPU counts
                 S = min(bsz, 1 << 16)
                 so.intersect(batch, so.VARIANTS["auto"], False, stream=stream, counts=counts, queue=queue, total=tot)
@@ -518,25 +654,43 @@ def run_setops(args, dist):
         totals = {k: r["intersection_total"] for k, r in res.items() if k.startswith(f"ov{ov}:")}
         assert len(set(totals.values())) == 1, totals
     best = max((r["pairs_per_s"], k) for k, r in res.items() if k.endswith(":count"))
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    hbm = peaks.get("hbm_gbs") or 6650.0
+    hbm, peak_src = peak_hbm()
     bk = res[best[1]]
-    line = {"metric": "set-intersection pairs/sec (2^24 Zipf(1.2) pairs)", "value": best[0], "unit": "pairs/s",
+    line = {"metric": f"set-intersection pairs/sec (2^{pairs_log2} Zipf(1.2) pairs)", "value": best[0],
+            "unit": "pairs/s",
             "best": best[1], "n_gpus": 1, "steps": len(overlaps), "warmup": 1, "higher_is_better": True,
             "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"set-intersection microbench, 2^{args.pairs_log2} pairs per overlap, "
+            "config": {"workload": f"set-intersection microbench, 2^{pairs_log2} pairs per overlap, "
                                    f"Zipf(1.2) lengths on [1, 65536], values in [0, 2^26)",
                        "batch_pairs": bsz, "overlaps": overlaps, "seed": args.seed,
                        "l2": "inputs larger than L2 (each batch holds ~14 GB of lists)"},
             "roofline": {"bound": "hbm", "achieved": bk["GB_per_s"], "peak": hbm, "unit": "GB/s",
-                         "frac": bk["GB_per_s"] / hbm, "traffic": None,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback"},
+                         "frac": bk["GB_per_s"] / hbm, "traffic": None, "peak_source": peak_src},
             "cpu_baseline": cpu, "gpu_launches": launches, "variants": res}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def run_batch(args, dist):
+    import torch
+
+    torch.cuda.set_device(dist.local)
+    line = batch_measure(args, args.steps, args.warmup)
+    print(json.dumps(line), flush=True)
+    return 1 if line["mismatched_graphs"] else 0
+
+
+def batch_summary(args) -> dict:
+    """The batched workload for the default line: graphs/s of the captured
+    launch, the sequential per-graph launches, their ratio and the number of
+    graphs whose counts differ (batched vs sequential)."""
+    line = batch_measure(args, 5, 3)
+    keep = ("value", "unit", "ms_per_step", "sequential_ms_per_step", "speedup_vs_sequential",
+            "oriented_edges_per_s", "mismatched_graphs", "total_triangles", "build_s")
+    return {"metric": line["metric"], **{k: line[k] for k in keep}, "graphs": line["config"]["graphs"],
+            "autotuned": line["config"]["autotuned"], "full_run": "python bench.py --workload batch"}
+
+
+def batch_measure(args, steps: int, warmup: int) -> dict:
     """Batched counting: 4096 graphs (n log-uniform in [1e3, 2e5], half BA with
     m in 2..16, half RMAT ef8) in one autotuned, CUDA-graph-captured persistent
     launch, against 4096 sequential per-graph launches of the plain kernel on
@@ -547,7 +701,6 @@ def run_batch(args, dist):
     from gary_b200 import autotune as at
     from gary_b200 import batch as B
 
-    torch.cuda.set_device(dist.local)
     t0 = time.perf_counter()
     specs = B.make_specs(args.graphs, seed=args.seed)
     batch = B.Batch.build(specs)
@@ -569,16 +722,18 @@ def run_batch(args, dist):
         with torch.cuda.stream(stream):
             tuned = at.autotune(batch.graph, one)
     exe = batch.capture(stream)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         exe.launch(stream)
     stream.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         exe.launch(stream)
     e1.record(stream)
     stream.synchronize()
-    ms_batch = e0.elapsed_time(e1) / args.steps
+    ms_batch = e0.elapsed_time(e1) / steps
+    from gary_b200._lib import check
+    check(L.gary_count_status(batch.graph.handle, stream.cuda_stream), "gary_count_status")
     bcounts = exe.counts.cpu().numpy().view(np.uint64).copy()
     # sequential baseline: the same graphs uploaded one by one, one launch each
     t1 = time.perf_counter()
@@ -590,13 +745,13 @@ def run_batch(args, dist):
     stream.synchronize()
     seq_build_s = time.perf_counter() - t1
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         with torch.cuda.stream(stream):
             for k, g in enumerate(graphs):
                 g.count_async(outs[k:k + 1], stream=stream)
     e1.record(stream)
     stream.synchronize()
-    ms_seq = e0.elapsed_time(e1) / args.steps
+    ms_seq = e0.elapsed_time(e1) / steps
     scounts = outs.cpu().numpy().view(np.uint64)
     direct, _ = batch.count()  # the batched count without the CUDA graph
     bad = np.nonzero(scounts != bcounts)[0]
@@ -611,24 +766,24 @@ def run_batch(args, dist):
                              "direct": int(direct[i]), "sequential": int(scounts[i]),
                              "oracle": O.tri_count(dp, di)})
     line = {"metric": "batched triangle count: graphs/s (4096 graphs, one captured launch)",
-            "value": len(specs) / (ms_batch / 1e3), "unit": "graphs/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": True, "dtype": "u32",
+            "value": len(specs) / (ms_batch / 1e3), "unit": "graphs/s", "n_gpus": 1, "steps": steps,
+            "warmup": warmup, "ms_per_step": ms_batch, "higher_is_better": True, "dtype": "u32",
             "data": "synthetic",
             "config": {"workload": f"{len(specs)} graphs, n log-uniform in [1e3, 2e5], even BA (m in 2..16), "
                                    f"odd RMAT ef8, seed {args.seed}",
-                       "vertices": inf["n"], "oriented_edges": inf["m"], "autotuned": tuned["config"]},
+                       "graphs": len(specs), "vertices": inf["n"], "oriented_edges": inf["m"],
+                       "autotuned": tuned["config"]},
             "sequential_ms_per_step": ms_seq, "speedup_vs_sequential": ms_seq / ms_batch,
             "oriented_edges_per_s": inf["m"] / (ms_batch / 1e3), "total_triangles": int(bcounts.sum()),
             "build_s": build_s, "sequential_build_s": seq_build_s,
             "autotune_trials": tuned["trials"], "mismatched_graphs": int(len(bad)), "mismatch_samples": mismatch}
-    print(json.dumps(line), flush=True)
-    if len(bad):
-        return 1
     exe.free()
     for g in graphs:
         g.free()
     batch.free()
-    return 0
+    at.apply({})
+    torch.cuda.empty_cache()
+    return line
 
 
 def run_patterns(args, dist):

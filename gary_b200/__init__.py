@@ -155,11 +155,24 @@ class Graph:
             raise ValueError("count_async needs a device tensor")
         check(load().gary_count_async(self._h, pattern, sched, _stream(stream), p), "gary_count_async")
 
+    def status(self, stream=None) -> int:
+        """Status of the last counting launch (gary_count_status): waits for
+        `stream` and returns GARY_OK, GARY_ERR_TIMEOUT or GARY_ERR_INTERNAL."""
+        return load().gary_count_status(self._h, _stream(stream))
+
+    def check_status(self, stream=None) -> None:
+        """Raise GaryError when the last counting launch reported a failure."""
+        check(self.status(stream), "gary_count_status")
+
     def last_stats(self) -> dict:
+        """Kernel time, tiles, CTA tiles per set path (bitmap, buckets, staged,
+        sampled), the error word and the triangle plan's probe count of the
+        last count (after its stream is synchronised)."""
         st = CountStats()
         check(load().gary_count_last_stats(self._h, C.byref(st)), "gary_count_last_stats")
         return {"kernel_ms": st.kernel_ms, "tiles": st.tiles, "cta_tiles": st.cta_tiles,
-                "variant_tiles": list(st.variant_tiles)}
+                "cta_path_tiles": dict(zip(("bitmap", "buckets", "staged", "sampled"), st.cta_path_tiles)),
+                "error": st.error, "work": st.work}
 
 
 class DeviceCsr:

@@ -19,6 +19,7 @@ GARY_ERR_OOM = -3
 GARY_ERR_INPUT = -4
 GARY_ERR_TIMEOUT = -5
 GARY_ERR_UNSUPPORTED = -6
+GARY_ERR_INTERNAL = -7
 
 GARY_INPUT_SYMMETRIC = 0x0
 GARY_INPUT_DAG = 0x1
@@ -79,7 +80,9 @@ class CountStats(C.Structure):
         ("kernel_ms", C.c_float),
         ("tiles", C.c_uint32),
         ("cta_tiles", C.c_uint32),
-        ("variant_tiles", C.c_uint32 * 4),
+        ("cta_path_tiles", C.c_uint32 * 4),  # bitmap, buckets, staged whole, sampled
+        ("error", C.c_uint32),
+        ("work", C.c_uint64),
     ]
 
 
@@ -103,6 +106,7 @@ SIGNATURES = {
     "gary_count_async": (_INT, [_P, _INT, _INT, _P, _P]),
     "gary_count_shard_async": (_INT, [_P, _INT, _INT, _U32, _U32, _P, _P]),
     "gary_count_last_stats": (_INT, [_P, C.POINTER(CountStats)]),
+    "gary_count_status": (_INT, [_P, _P]),
     "gary_count_triangles_noalloc": (_INT, [_P, _P, _P, _U32, _P, _P]),
     "gary_tune": (_INT, [C.c_char_p, _U64]),
     "gary_batch_upload": (_INT, [_P, _U32, _P, _P, _U32, _U64, _U32, _P, C.POINTER(_P)]),

@@ -91,9 +91,20 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     return LIB
 
 
+def reference_tree() -> Path | None:
+    """The reference's source tree for the oracle build: $GARY_REF_TREE, else a
+    `reference` directory beside this repository, when either holds its
+    sources (src/Graph.cpp)."""
+    for cand in (os.environ.get("GARY_REF_TREE"), ROOT.parent / "reference"):
+        if cand and (Path(cand) / "src" / "Graph.cpp").exists():
+            return Path(cand)
+    return None
+
+
 def build_oracle(verbose: bool = False) -> None:
     """Compile the CPU oracle, and the reference's own code when its tree is present."""
-    cmd = ["make", "-s", "-C", str(ROOT / "oracle"), f"PYTHON={sys.executable}", "all"]
+    ref = reference_tree()
+    cmd = ["make", "-s", "-C", str(ROOT / "oracle"), f"PYTHON={sys.executable}", f"REF={ref or ''}", "all"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")

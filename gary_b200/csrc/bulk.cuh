@@ -67,9 +67,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity.  Returns false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kSpinLimit; ++i)
+// Bounded wait for the phase with the given parity: at most `polls` polls
+// of try_wait (0 gives up at once).  Returns false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  uint32_t polls = kSpinLimit) {
+  for (uint32_t i = 0; i < polls; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

@@ -340,6 +340,18 @@ PlanParams tuned_params() {
   return g_tuning;
 }
 
+// GARY_OK, or the status the error word of a counting launch stands for.
+int launch_status(uint32_t err) {
+  if (!err) return GARY_OK;
+  if (err & kLaunchErrTableFull) {
+    set_error("a shared-memory table of the counting kernel overflowed (error word 0x%x): the count "
+              "is incomplete", err);
+    return GARY_ERR_INTERNAL;
+  }
+  set_error("a bounded device wait expired (error word 0x%x): the count is incomplete", err);
+  return GARY_ERR_TIMEOUT;
+}
+
 }  // namespace gary
 
 using gary::guarded;
@@ -349,8 +361,13 @@ extern "C" int gary_tune(const char *key, uint64_t value) {
   std::lock_guard<std::mutex> lk(gary::g_tuning_mu);
   gary::PlanParams &p = gary::g_tuning;
   const std::string k(key);
+  const bool pow2 = value && !(value & (value - 1));
   if (k == "warp_tile_cost") p.warp_tile_cost = value;  // 0: from the work
   else if (k == "cta_tile_cost" && value > 0) p.cta_tile_cost = value;
+  else if (k == "warp_cap" && value >= 8 && value <= gary::kWarpTableSlots / 2) p.warp_cap = (uint32_t)value;
+  else if (k == "cta_set_words" && (value == 0 || (pow2 && value >= 64 && value <= gary::kTcWarps * gary::kWarpTableSlots)))
+    p.cta_set_words = (uint32_t)value;
+  else if (k == "stage_wait_polls" && value <= gary::kSpinLimit) p.stage_polls = (uint32_t)value;
   else if (k == "vertex_overhead") p.vertex_overhead = value;
   else if (k == "min_blocks" && (value == 0 || value == 2 || value == 3)) p.min_blocks = (uint32_t)value;
   else if (k == "pool_keep_bytes") gary::set_pool_keep_bytes(value);
@@ -581,17 +598,10 @@ extern "C" int gary_count(gary_graph *g, int pattern, int sched, void *stream, u
     GARY_TRY(gary::count_async(g, pattern, sched, s, g->result.p));
     unsigned long long h = 0;
     gary::SchedState st{};
-    const gary::SchedState *dst = nullptr;
-    if (pattern == GARY_PATTERN_TRIANGLE) dst = g->plans[gary::plan_slot(pattern, sched)]->sched.p;
-    else if (pattern == GARY_PATTERN_4CLIQUE) dst = g->k4_plan->sched.p;
-    else dst = g->c4_plan->sched.p;
     GARY_CUDA(cudaMemcpyAsync(&h, g->result.p, sizeof(h), cudaMemcpyDeviceToHost, s));
-    GARY_CUDA(cudaMemcpyAsync(&st, dst, sizeof(st), cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaMemcpyAsync(&st, g->last_sched, sizeof(st), cudaMemcpyDeviceToHost, s));
     GARY_CUDA(cudaStreamSynchronize(s));
-    if (st.error) {
-      gary::set_error("a bounded device wait expired (error word 0x%x)", st.error);
-      return GARY_ERR_TIMEOUT;
-    }
+    GARY_TRY(gary::launch_status(st.error));
     *out = h;
     return GARY_OK;
   });
@@ -605,8 +615,26 @@ extern "C" int gary_count_shard_async(gary_graph *g, int pattern, int sched, uin
   });
 }
 
+extern "C" int gary_count_status(gary_graph *g, void *stream) {
+  GARY_CHECK_ARG(g != nullptr, "graph is NULL");
+  GARY_CHECK_ARG(g->last_sched != nullptr, "no count has been launched on this graph");
+  return guarded("gary_count_status", [&] {
+    cudaStream_t s = gary::as_stream(stream);
+    gary::SchedState st{};
+    GARY_CUDA(cudaMemcpyAsync(&st, g->last_sched, sizeof(st), cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaStreamSynchronize(s));
+    return gary::launch_status(st.error);
+  });
+}
+
 extern "C" int gary_count_last_stats(gary_graph *g, gary_count_stats *out) {
   GARY_CHECK_ARG(g != nullptr && out != nullptr, "NULL argument");
+  if (g->last_sched) {
+    gary::SchedState st{};
+    GARY_CUDA(cudaMemcpy(&st, g->last_sched, sizeof(st), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 4; ++k) g->last.cta_path_tiles[k] = st.cta_path[k];
+    g->last.error = st.error;
+  }
   if (g->last_timed) {
     float ms = 0.f;
     cudaError_t e = cudaEventElapsedTime(&ms, g->ev0, g->ev1);

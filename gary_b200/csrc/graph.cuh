@@ -26,6 +26,7 @@ struct gary_count_plan;  // tc.cu: cached tile lists per (pattern, sched)
 
 namespace gary {
 struct PatternPlan;  // patterns.cu: 4-clique / 4-cycle plans
+struct SchedState;   // tc.cuh: scheduler and error words of a counting launch
 struct PaddedCSR {
   uint32_t n = 0;
   uint64_t m = 0;      // stored ids
@@ -73,6 +74,7 @@ struct gary_graph {
   gary::DevBuf<unsigned long long> result;  // device word for gary_count
   gary_count_stats last{};
   bool last_timed = false;  // ev0/ev1 bracket the last counting kernel
+  const gary::SchedState *last_sched = nullptr;  // scheduler words of the last counting launch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   gary::GraphView view() const { return gary::GraphView{n, dag.row.p, dag.adj.p, true}; }

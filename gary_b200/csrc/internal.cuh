@@ -15,6 +15,14 @@ constexpr uint32_t kSentinel = 0xFFFFFFFFu;  // list padding; never a vertex id
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
+// Bits of a counting launch's error word (SchedState::error), zeroed before
+// every launch and read back by gary_count and gary_count_status.
+enum : uint32_t {
+  kLaunchErrStageWait = 1u,   // a bulk-copy wait gave up after its poll limit
+  kLaunchErrStageDrain = 2u,  // the drain wait after it gave up too: that CTA stopped work
+  kLaunchErrTableFull = 4u,   // a shared-memory table had no free slot (capacity rule broken)
+};
+
 // ---- error reporting (thread-local message; see gary_last_error) --------
 void set_error(const char *fmt, ...);
 void clear_error();

@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kNaWarps * 32)
         const BitmapSet st = build_bitmap(au, d, lo, span, tab, lane, 32, sync);
         cnt = walk_out_lists(indptr, colidx, deg, n, au, d, lane, st);
       } else if (2 * d <= kNaSlots) {
-        const BucketSet st = build_buckets(au, d, lo, span, tab, kNaSlots, lane, 32, sync);
+        const BucketSet st = build_buckets(au, d, lo, span, tab, kNaSlots, lane, 32, sync, nullptr);
         cnt = walk_out_lists(indptr, colidx, deg, n, au, d, lane, st);
       } else {
         const GlobalSearchSet st{au, d, lo, span};

@@ -116,10 +116,12 @@ __device__ __forceinline__ void c4_wedges(const GraphView &s, const uint32_t *__
 }
 
 // Counter map in shared memory: increments c(w) and returns the old value.
+// The plan keeps the map at most half full; a probe that finds every slot
+// taken (a broken capacity rule) sets kLaunchErrTableFull and counts nothing.
 __device__ __forceinline__ uint32_t map_incr(uint32_t *keys, uint32_t *vals, uint32_t mask, int shift,
-                                             uint32_t w) {
+                                             uint32_t w, unsigned *err) {
   uint32_t h = (w * kHashMul) >> shift;
-  while (true) {
+  for (uint32_t i = 0; i <= mask; ++i) {
     const uint32_t k = keys[h];
     if (k == w) return atomicAdd(&vals[h], 1u);
     if (k == kSentinel) {
@@ -128,6 +130,8 @@ __device__ __forceinline__ uint32_t map_incr(uint32_t *keys, uint32_t *vals, uin
     }
     h = (h + 1) & mask;
   }
+  atomicOr(err, kLaunchErrTableFull);
+  return 0;
 }
 
 __global__ void __launch_bounds__(kPWarps * 32)
@@ -156,7 +160,7 @@ __global__ void __launch_bounds__(kPWarps * 32)
       }
       __syncwarp();
       c4_wedges(s, dplus, au, u, 0, pre, 32, lane, [&](uint32_t w) {
-        acc += map_incr(keys, vals, kPSlots - 1, 32 - 10, w);
+        acc += map_incr(keys, vals, kPSlots - 1, 32 - 10, w, &sched->error);
       });
       __syncwarp();
     }
@@ -178,9 +182,9 @@ static_assert(kMidWedges < 65536, "16-bit medium counts");
 
 // As map_incr, with the count of slot h in half h & 1 of word h / 2 of vals2.
 __device__ __forceinline__ uint32_t map_incr16(uint32_t *keys, uint32_t *vals2, uint32_t mask, int shift,
-                                               uint32_t w) {
+                                               uint32_t w, unsigned *err) {
   uint32_t h = (w * kHashMul) >> shift;
-  while (true) {
+  for (uint32_t i = 0; i <= mask; ++i) {
     const uint32_t k = keys[h];
     bool hit = k == w;
     if (!hit && k == kSentinel) {
@@ -193,6 +197,8 @@ __device__ __forceinline__ uint32_t map_incr16(uint32_t *keys, uint32_t *vals2, 
     }
     h = (h + 1) & mask;
   }
+  atomicOr(err, kLaunchErrTableFull);
+  return 0;
 }
 
 __global__ void __launch_bounds__(kMidThreads, 2)
@@ -222,7 +228,7 @@ __global__ void __launch_bounds__(kMidThreads, 2)
       k = __shfl_sync(kFull, k, 0);
       if (k >= pre) break;
       c4_wedges(s, dplus, au, u, k, min(k + 32, pre), 32, lane, [&](uint32_t w) {
-        acc += map_incr16(keys, vals, kMidSlots - 1, 32 - kMidLog, w);
+        acc += map_incr16(keys, vals, kMidSlots - 1, 32 - kMidLog, w, &sched->error);
       });
     }
     __syncthreads();
@@ -525,22 +531,32 @@ static_assert(2 * (1u << kK4WarpLog) + kK4WarpMaxD * (kK4WarpMaxD / 32) <= kK4Wa
               "warp region too small");
 static_assert((1u << kK4MidLog) >= 2 * kK4MidMaxD, "mid hash too small");
 
+// Position hash of N+(u) (ids are distinct; the table is at least twice the
+// list).  Both loops visit each slot at most once: a full table (a broken
+// capacity rule) sets kLaunchErrTableFull on insert and misses on lookup.
 __device__ __forceinline__ void pos_insert(uint32_t *keys, uint32_t *pos, uint32_t mask, int shift,
-                                           uint32_t x, uint32_t p) {
+                                           uint32_t x, uint32_t p, unsigned *err) {
   uint32_t h = (x * kHashMul) >> shift;
-  while (atomicCAS(&keys[h], kSentinel, x) != kSentinel) h = (h + 1) & mask;  // ids are distinct
-  pos[h] = p;
+  for (uint32_t i = 0; i <= mask; ++i) {
+    if (atomicCAS(&keys[h], kSentinel, x) == kSentinel) {
+      pos[h] = p;
+      return;
+    }
+    h = (h + 1) & mask;
+  }
+  atomicOr(err, kLaunchErrTableFull);
 }
 
 __device__ __forceinline__ int pos_find(const uint32_t *keys, const uint32_t *pos, uint32_t mask,
                                         int shift, uint32_t x) {
   uint32_t h = (x * kHashMul) >> shift;
-  while (true) {
+  for (uint32_t i = 0; i <= mask; ++i) {
     const uint32_t k = keys[h];
     if (k == kSentinel) return -1;  // first: x may itself be the padding value
     if (k == x) return (int)pos[h];
     h = (h + 1) & mask;
   }
+  return -1;
 }
 
 // 4-cliques with lowest vertex u; `nthreads` threads (one warp or the CTA)
@@ -549,7 +565,7 @@ __device__ __forceinline__ int pos_find(const uint32_t *keys, const uint32_t *po
 template <typename Sync>
 __device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t *keys, uint32_t *pos,
                                         uint32_t max_log, uint32_t *rows, uint32_t tid,
-                                        uint32_t nthreads, Sync sync) {
+                                        uint32_t nthreads, Sync sync, unsigned *err) {
   const int lane = tid & 31;
   const uint2 ru = g.row[u];
   const uint32_t d = ru.y;
@@ -559,7 +575,7 @@ __device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t
   if (l > (int)max_log) l = (int)max_log;
   const uint32_t mask = (1u << l) - 1;
   const int shift = 32 - l;
-  for (uint32_t i = tid; i < d; i += nthreads) pos_insert(keys, pos, mask, shift, au[i], i);
+  for (uint32_t i = tid; i < d; i += nthreads) pos_insert(keys, pos, mask, shift, au[i], i, err);
   sync();
   const uint32_t maxu = au[d - 1];
   // rows: 32 rows per warp step.  Each N+(v) is read as 32-byte octets from
@@ -620,7 +636,7 @@ __device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t
 template <int THREADS, int HLOG, uint32_t ROWW>
 __global__ void __launch_bounds__(THREADS)
     k_k4_cta(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
-             uint32_t *__restrict__ pool, uint64_t pool_words, uint32_t *counter,
+             uint32_t *__restrict__ pool, uint64_t pool_words, uint32_t *counter, unsigned *err,
              unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t sm[];
   __shared__ uint32_t s_idx;
@@ -638,7 +654,7 @@ __global__ void __launch_bounds__(THREADS)
     const uint32_t d = g.row[u].y;
     const uint64_t words = (uint64_t)d * ((d + 31) >> 5);
     uint32_t *rows = words <= ROWW ? srows : pool + (uint64_t)blockIdx.x * pool_words;
-    cnt += k4_vertex(g, u, keys, pos, HLOG, rows, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+    cnt += k4_vertex(g, u, keys, pos, HLOG, rows, threadIdx.x, blockDim.x, [] { __syncthreads(); }, err);
   }
   cnt = warp_sum_u64(cnt);
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
@@ -647,7 +663,7 @@ __global__ void __launch_bounds__(THREADS)
 // Warp vertices: each warp in its own region of shared memory, 32 vertices per claim.
 __global__ void __launch_bounds__(kK4WarpCtaWarps * 32)
     k_k4_warp(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
-              uint32_t *counter, unsigned long long *__restrict__ out) {
+              uint32_t *counter, unsigned *err, unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t sm[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *keys = sm + warp * kK4WarpWords, *pos = keys + (1u << kK4WarpLog),
@@ -666,7 +682,7 @@ __global__ void __launch_bounds__(kK4WarpCtaWarps * 32)
     const uint32_t myu = lane < nb ? list[i0 + lane] : 0u;
     for (uint32_t q = 0; q < nb; ++q)
       cnt += k4_vertex(g, __shfl_sync(kFull, myu, q), keys, pos, kK4WarpLog, rows, lane, 32,
-                       [] { __syncwarp(); });
+                       [] { __syncwarp(); }, err);
   }
   cnt = warp_sum_u64(cnt);
   if (lane == 0 && cnt) atomicAdd(out, cnt);
@@ -883,20 +899,21 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
       return GARY_ERR_INVALID;
     }
     big<<<grid, kK4BigThreads, smem_big, s>>>(gv, plan->big.p, b0, b1, plan->cursors.p, pool_words,
-                                              &st->next_cta, d_out);
+                                              &st->next_cta, &st->error, d_out);
   }
   if (m1 > m0)
     mid<<<std::min<unsigned>((unsigned)(sm_count() * per_mid), m1 - m0), kK4MidThreads, smem_mid, s>>>(
-        gv, plan->mid.p, m0, m1, nullptr, 0, &st->next_aux, d_out);
+        gv, plan->mid.p, m0, m1, nullptr, 0, &st->next_aux, &st->error, d_out);
   if (w1 > w0)
     k_k4_warp<<<(unsigned)(sm_count() * per_warp), kK4WarpCtaWarps * 32, smem_warp, s>>>(
-        gv, plan->light.p, w0, w1, &st->next_warp, d_out);
+        gv, plan->light.p, w0, w1, &st->next_warp, &st->error, d_out);
   GARY_CUDA(cudaGetLastError());
   GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
   g->last.tiles = (b1 - b0) + (m1 - m0) + (w1 - w0);
   g->last.cta_tiles = (b1 - b0) + (m1 - m0);
   g->last_timed = true;
+  g->last_sched = st;
   return GARY_OK;
 }
 
@@ -1022,6 +1039,7 @@ int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   g->last.tiles = (t1 - t0) + (m1 - m0) + (l1 - l0);
   g->last.cta_tiles = (t1 - t0) + (m1 - m0);
   g->last_timed = true;
+  g->last_sched = plan->sched.p;
   return GARY_OK;
 }
 

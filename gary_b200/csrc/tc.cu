@@ -19,13 +19,11 @@
 // Work is cut into tiles of bounded probe count over the in-edge index and
 // served by a persistent scheduler: CTA tiles (large N+(v)) first, then warp
 // tiles.
-#include <cub/cub.cuh>
 #include <thrust/binary_search.h>
 #include <thrust/copy.h>
 #include <thrust/execution_policy.h>
 #include <thrust/fill.h>
 #include <thrust/iterator/counting_iterator.h>
-#include <thrust/iterator/reverse_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
 #include <thrust/reduce.h>
 #include <thrust/scan.h>
@@ -54,85 +52,65 @@ inline unsigned grid_for(uint64_t items) {
   return (unsigned)std::max<uint64_t>(std::min(b, cap), 1);
 }
 
-inline int bits_for(uint64_t x) {
-  int b = 0;
-  while (b < 64 && (x - 1) >> b) ++b;
-  return std::max(b, 1);
-}
-
 __host__ __device__ __forceinline__ uint64_t min_u64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
-struct MinU64 {
-  __host__ __device__ uint64_t operator()(uint64_t a, uint64_t b) const { return a < b ? a : b; }
-};
-
-// One candidate per padded word w of N+(u): the suffix after v = adj[w].
-// Words without a record get the key n - 1: in rank ids the top vertex has
-// no higher neighbour, so no record ever targets it, and the keys of an
-// n = 2^k graph fit k bits (one radix pass fewer than with the key n).
-__global__ void k_in_candidates(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
-                                const uint32_t *__restrict__ rowid, uint64_t words, uint32_t n,
-                                uint32_t *__restrict__ keys, uint2 *__restrict__ vals) {
-  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words;
-       w += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t u = rowid[w];
-    const uint2 r = row[u];
-    const uint64_t pos = w - (uint64_t)r.x * 4;
-    uint32_t key = n - 1;
-    uint2 val = make_uint2(0, 0);
-    if (pos < r.y) {
-      const uint32_t v = adj[w];
-      const uint32_t rem = r.y - (uint32_t)pos - 1;
-      if (rem && row[v].y) {
-        key = v;
-        val = make_uint2((uint32_t)(w + 1), rem);
+// The in-edge index is the transpose of the DAG: for every oriented edge
+// u -> v whose suffix S(u,v) (the part of N+(u) after v) is non-empty, and
+// with d+(v) > 0, one record {first word of S(u,v), |S(u,v)|} in v's group.
+// Built without a sort: a count pass gives each record its slot in its
+// target's group (the old value of an atomic counter), a scan turns the
+// counts into group offsets, and a fill pass writes every record to its
+// place.  Both passes walk the rows of 32 consecutive vertices per warp,
+// flattened across the lanes (rows are short on average), so adj is read in
+// order.  Within a group the records come in no particular order; the count
+// does not depend on it.
+template <typename F>
+__device__ __forceinline__ void walk_records(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
+                                             uint32_t n, F f) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c * 32 < n; c += nwarps) {
+    const uint64_t u = c * 32 + lane;
+    const uint2 r = u < n ? row[u] : make_uint2(0, 0);
+    const uint32_t incl = warp_inclusive_sum(r.y, lane);
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    for (uint32_t pb = 0; pb < total; pb += 32) {
+      const uint32_t p = pb + lane;
+      const int o = warp_owner(incl, p);
+      const uint32_t ox = __shfl_sync(kFull, incl - r.y, o);
+      const uint32_t base4 = __shfl_sync(kFull, r.x, o);
+      const uint32_t len = __shfl_sync(kFull, r.y, o);
+      if (p < total) {
+        const uint32_t pos = p - ox;
+        const uint32_t rem = len - pos - 1;
+        const uint64_t w = (uint64_t)base4 * 4 + pos;
+        const uint32_t v = adj[w];
+        if (rem && row[v].y) f(w, v, rem);
       }
     }
-    keys[w] = key;
-    vals[w] = val;
   }
 }
 
-// first index i with keys[i] >= x in a sorted array (one thread)
-__global__ void k_first_geq(const uint32_t *__restrict__ keys, uint64_t len, uint32_t x,
-                            uint64_t *__restrict__ out) {
-  uint64_t b = 0, e = len;
-  while (b < e) {
-    const uint64_t m = (b + e) >> 1;
-    if (keys[m] < x) b = m + 1;
-    else e = m;
-  }
-  *out = b;
+__global__ void k_in_count(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj, uint32_t n,
+                           uint32_t *__restrict__ cnt, unsigned long long *__restrict__ work,
+                           uint32_t *__restrict__ slot) {
+  walk_records(row, adj, n, [&](uint64_t w, uint32_t v, uint32_t rem) {
+    slot[w] = atomicAdd(&cnt[v], 1u);
+    atomicAdd(&work[v], (unsigned long long)rem);
+  });
 }
 
-__global__ void k_in_heads(const uint32_t *__restrict__ keys, uint64_t m,
-                           uint64_t *__restrict__ inptr) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t v = keys[i];
-    if (i == 0 || keys[i - 1] != v) inptr[v] = i;
-  }
+__global__ void k_in_fill(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj, uint32_t n,
+                          const uint64_t *__restrict__ inptr, const uint32_t *__restrict__ slot,
+                          uint2 *__restrict__ inedge) {
+  walk_records(row, adj, n, [&](uint64_t w, uint32_t v, uint32_t rem) {
+    inedge[inptr[v] + slot[w]] = make_uint2((uint32_t)(w + 1), rem);
+  });
 }
 
-// work[v] = sum of suffix lengths of v's in-edges (segmented warp scan; keys sorted).
-__global__ void k_in_work(const uint32_t *__restrict__ keys, const uint2 *__restrict__ vals,
-                          uint64_t m, unsigned long long *__restrict__ work) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < m; base += stride) {
-    const uint64_t i = base + threadIdx.x;
-    const bool ok = i < m;
-    const uint32_t v = ok ? keys[i] : 0xFFFFFFFFu;
-    unsigned long long x = ok ? vals[i].y : 0ull;
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned long long t = __shfl_up_sync(kFull, x, o);
-      const uint32_t tv = __shfl_up_sync(kFull, v, o);
-      if (lane >= o && tv == v) x += t;
-    }
-    const uint32_t nv = __shfl_down_sync(kFull, v, 1);
-    if (ok && (lane == 31 || nv != v) && x) atomicAdd(&work[v], x);
-  }
-}
+struct U32ToU64 {
+  __host__ __device__ uint64_t operator()(uint32_t x) const { return x; }
+};
 
 // pcost (optional): predicted cycles of a warp-class vertex, with tile target
 // tw_pred in the same unit; without it, costs are probe counts.
@@ -311,58 +289,29 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
   }
   ScratchAlloc pol_alloc{s};
   auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
-  DevBuf<uint32_t> keys, keys2;
-  DevBuf<uint2> vals, vals2;
-  {
-    DevBuf<uint32_t> rowid;
-    GARY_TRY(padded_rowid(g->dag, rowid, s));
-    GARY_TRY(keys.alloc(W, s));
-    GARY_TRY(vals.alloc(W, s));
-    k_in_candidates<<<grid_for(W), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, rowid.p, W, n, keys.p,
-                                                     vals.p);
-    GARY_CUDA(cudaGetLastError());
-  }
-  GARY_TRY(keys2.alloc(W, s));
-  GARY_TRY(vals2.alloc(W, s));
-  {
-    cub::DoubleBuffer<uint32_t> kb(keys.p, keys2.p);
-    cub::DoubleBuffer<uint2> vb(vals.p, vals2.p);
-    size_t tmp = 0;
-    const int eb = bits_for((uint64_t)n);  // keys <= n - 1
-    GARY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kb, vb, W, 0, eb, s));
-    DevBuf<uint8_t> t;
-    GARY_TRY(t.alloc(tmp, s));
-    GARY_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kb, vb, W, 0, eb, s));
-    if (kb.Current() != keys.p) std::swap(keys, keys2);
-    if (vb.Current() != vals.p) std::swap(vals, vals2);
-  }
-  keys2.release();
-  vals2.release();
-  // records = number of keys < n - 1 (the rest carry the "no record" key n - 1)
-  uint64_t m = 0;
-  {
-    DevBuf<uint64_t> pos;
-    GARY_TRY(pos.alloc(1, s));
-    k_first_geq<<<1, 1, 0, s>>>(keys.p, W, n - 1, pos.p);
-    GARY_CUDA(cudaGetLastError());
-    GARY_CUDA(cudaMemcpyAsync(&m, pos.p, 8, cudaMemcpyDeviceToHost, s));
-    GARY_CUDA(cudaStreamSynchronize(s));
-  }
-  in.records = m;
-  GARY_TRY(in.inptr.alloc_persistent((uint64_t)n + 1));
-  thrust::fill(pol, in.inptr.p, in.inptr.p + n + 1, m);
-  if (m) k_in_heads<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, in.inptr.p);
-  auto rb = thrust::make_reverse_iterator(in.inptr.p + n + 1);
-  thrust::inclusive_scan(pol, rb, rb + n + 1, rb, MinU64());
-  GARY_TRY(in.inedge.alloc_persistent(std::max<uint64_t>(m, 1)));
-  if (m)
-    GARY_CUDA(cudaMemcpyAsync(in.inedge.p, vals.p, m * sizeof(uint2), cudaMemcpyDeviceToDevice, s));
+  DevBuf<uint32_t> cnt, slot;
+  GARY_TRY(cnt.alloc((uint64_t)n + 1, s));
+  GARY_TRY(slot.alloc(std::max<uint64_t>(W, 1), s));
   GARY_TRY(in.work.alloc_persistent(n));
+  GARY_CUDA(cudaMemsetAsync(cnt.p, 0, ((uint64_t)n + 1) * 4, s));
   GARY_CUDA(cudaMemsetAsync(in.work.p, 0, (uint64_t)n * 8, s));
-  if (m)
-    k_in_work<<<grid_for(m), kThreads, 0, s>>>(keys.p, vals.p, m,
-                                              reinterpret_cast<unsigned long long *>(in.work.p));
+  const unsigned grid = grid_for((uint64_t)n);  // one warp per 32 rows
+  k_in_count<<<grid, kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, n, cnt.p,
+                                       reinterpret_cast<unsigned long long *>(in.work.p), slot.p);
   GARY_CUDA(cudaGetLastError());
+  GARY_TRY(in.inptr.alloc_persistent((uint64_t)n + 1));
+  auto wide = thrust::make_transform_iterator(cnt.p, U32ToU64());
+  thrust::exclusive_scan(pol, wide, wide + n + 1, in.inptr.p, 0ull);
+  uint64_t m = 0;
+  GARY_CUDA(cudaMemcpyAsync(&m, in.inptr.p + n, 8, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaStreamSynchronize(s));
+  cnt.release();
+  in.records = m;
+  GARY_TRY(in.inedge.alloc_persistent(std::max<uint64_t>(m, 1)));
+  if (m) {
+    k_in_fill<<<grid, kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, n, in.inptr.p, slot.p, in.inedge.p);
+    GARY_CUDA(cudaGetLastError());
+  }
   in.total_work = thrust::reduce(pol, in.work.p, in.work.p + n, 0ull);
   return GARY_OK;
 }
@@ -569,12 +518,29 @@ __device__ __forceinline__ uint32_t cta_walk(const uint4 *__restrict__ adj4,
   return cnt;
 }
 
+// How CTA tiles hold N+(v): `words` shared words for the set (a multiple of
+// 4, at most the CTA's buffer) and the poll limit of the first wait for a
+// staging copy.
+struct CtaSetCfg {
+  uint32_t words;
+  uint32_t polls;
+};
+
+// One CTA tile.  N+(v) goes into the cheapest set that fits `cfg.words`
+// shared words: a bitmap of its id span, 4-slot hash buckets (d <= words/2),
+// the sorted list staged whole by a bulk copy (d <= words; searched in
+// shared memory only), or `words` evenly spaced samples of the list for the
+// two-phase search (phase 2 in HBM).  Adds the tile's count to cnt_total.
+// Returns false when a staging copy did not land within the drain wait: the
+// CTA must then stop touching shared memory (the copy may still arrive), so
+// the caller abandons its remaining work; the error word records it.
 template <int WARPS>
-__device__ uint32_t cta_tile(const GraphView &g, const uint2 *__restrict__ inedge,
-                             const uint64_t *__restrict__ inptr, const Tile &t, uint32_t *smem,
-                             uint32_t *chunk, uint64_t *bar, uint32_t &phase, unsigned *err,
-                             const uint32_t *gid, unsigned long long *gcount) {
-  constexpr uint32_t S = WARPS * kWarpTableSlots;  // shared words
+__device__ bool cta_tile(const GraphView &g, const uint2 *__restrict__ inedge,
+                         const uint64_t *__restrict__ inptr, const Tile &t, uint32_t *smem,
+                         uint32_t *chunk, uint64_t *bar, uint32_t &phase, const CtaSetCfg &cfg,
+                         SchedState *sched, const uint32_t *gid, unsigned long long *gcount,
+                         unsigned long long &cnt_total) {
+  const uint32_t S = cfg.words;
   const int lane = threadIdx.x & 31;
   const uint32_t v = t.v0;
   const uint2 rv = g.row[v];
@@ -586,38 +552,50 @@ __device__ uint32_t cta_tile(const GraphView &g, const uint2 *__restrict__ inedg
   const uint32_t lo = av[0], span = av[d - 1] - lo;
   auto sync = [] { __syncthreads(); };
   if (threadIdx.x == 0) *chunk = 0;
-  uint32_t cnt = 0;
+  uint32_t cnt = 0, path;
   if (span <= bitmap_max_span(S)) {
+    path = kPathBitmap;
     const BitmapSet st = build_bitmap(av, d, lo, span, smem, threadIdx.x, blockDim.x, sync);
     cnt = cta_walk<WARPS>(adj4, inedge, kb, ke, chunk, lane, st);
   } else if (2 * d <= S) {
-    const BucketSet st = build_buckets(av, d, lo, span, smem, S, threadIdx.x, blockDim.x, sync);
+    path = kPathBuckets;
+    const BucketSet st =
+        build_buckets(av, d, lo, span, smem, S, threadIdx.x, blockDim.x, sync, &sched->error);
     cnt = cta_walk<WARPS>(adj4, inedge, kb, ke, chunk, lane, st);
   } else {
-    // N+(v) staged whole (bulk copy) or sampled into shared memory; two-phase search
     if (d <= S) {
+      // the whole list by one bulk copy (lists start 32-byte aligned and are
+      // padded to whole octets, so the 16-byte-rounded size stays in the list)
+      path = kPathStaged;
       if (threadIdx.x == 0) bulk_stage(smem, av, ((d + 3) / 4) * 16, bar);
-      __syncthreads();
-      if (!mbar_wait_bounded(bar, phase)) {
-        if (threadIdx.x == 0) atomicOr(err, 1u);
-        mbar_wait_bounded(bar, phase);  // drain the copy before leaving
+      bool ok = mbar_wait_bounded(bar, phase, cfg.polls);
+      if (!ok) {
+        atomicOr(&sched->error, kLaunchErrStageWait);
+        ok = mbar_wait_bounded(bar, phase);  // drain the copy before going on
+      }
+      if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(&sched->error, kLaunchErrStageDrain);
+        return false;
       }
       phase ^= 1;
     } else {
+      path = kPathSampled;
       for (uint32_t i = threadIdx.x; i < S; i += blockDim.x) smem[i] = av[(uint64_t)i * d / S];
       __syncthreads();
     }
     const SearchSet st{av, smem, d, S, lo, span};
     cnt = cta_walk<WARPS>(adj4, inedge, kb, ke, chunk, lane, st);
   }
+  if (threadIdx.x == 0) atomicAdd(&sched->cta_path[path], 1u);
   if (gcount) {
     const unsigned long long tw = warp_sum_u64(cnt);
     if (lane == 0 && tw) atomicAdd(&gcount[gid[v]], tw);
   }
+  cnt_total += cnt;
   // the next tile rewrites shared memory, possibly through the async proxy
   fence_proxy_async_smem();
   __syncthreads();
-  return cnt;
+  return true;
 }
 
 // Sorted copy of N+(v) in shared memory, binary-searched (variant SEARCH).
@@ -657,6 +635,7 @@ struct VertexCtl {
   unsigned long long *cycles;  // clock64 cycles spent per middle vertex
   const uint32_t *gid;         // batches: graph of each middle vertex
   unsigned long long *gcount;  // batches: per-graph counts
+  unsigned *err;               // the launch's error word
 };
 
 // Batches: add a warp's count for middle vertex v to its graph's total.
@@ -695,7 +674,7 @@ __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 
     const BitmapSet st = build_bitmap(av, d, lo, span, tab, lane, 32, sync);
     c = walk_range(adj4, inedge, kb, ke, lane, st);
   } else if (var == kVarHash) {
-    const BucketSet st = build_buckets(av, d, lo, span, tab, kWarpTableSlots, lane, 32, sync);
+    const BucketSet st = build_buckets(av, d, lo, span, tab, kWarpTableSlots, lane, 32, sync, ctl.err);
     c = walk_range(adj4, inedge, kb, ke, lane, st);
   } else if (var == kVarSearch) {
     for (uint32_t i = lane; i < d; i += 32) tab[i] = av[i];
@@ -718,7 +697,8 @@ template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     k_tc_mid(GraphView g, const uint2 *__restrict__ inedge, const uint64_t *__restrict__ inptr,
              const uint32_t *__restrict__ light, const Tile *__restrict__ tiles, uint32_t n_cta,
-             TileRange rng, SchedState *sched, unsigned long long *__restrict__ out, VertexCtl ctl) {
+             TileRange rng, SchedState *sched, unsigned long long *__restrict__ out, VertexCtl ctl,
+             CtaSetCfg cfg) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint64_t bar;
   __shared__ uint32_t s_tile, s_chunk;
@@ -733,6 +713,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   uint32_t phase = 0;
 
   // phase 1: CTA tiles (N+(v) does not fit a warp's set)
+  bool alive = true;
   while (true) {
     if (threadIdx.x == 0) s_tile = rng.cta_lo + atomicAdd(&sched->next_cta, 1u);
     __syncthreads();
@@ -740,14 +721,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     __syncthreads();
     if (t >= rng.cta_hi) break;
     const Tile tl = tiles[t];
-    cnt += cta_tile<WARPS>(g, inedge, inptr, tl, smem, &s_chunk, &bar, phase, &sched->error,
-                           ctl.gid, ctl.gcount);
+    if (!cta_tile<WARPS>(g, inedge, inptr, tl, smem, &s_chunk, &bar, phase, cfg, sched, ctl.gid,
+                         ctl.gcount, cnt)) {
+      alive = false;  // a staging copy may still land in shared memory: no more work here
+      break;
+    }
   }
 
   // phase 2: warp tiles, each warp on its own slots
   uint32_t *tab = smem + warp * kWarpTableSlots;
   const Tile *wt = tiles + n_cta;
-  while (true) {
+  while (alive) {
     uint32_t t = 0;
     if (lane == 0) t = rng.warp_lo + atomicAdd(&sched->next_warp, 1u);
     t = __shfl_sync(kFull, t, 0);
@@ -769,7 +753,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
 
   cnt = warp_sum_u64(cnt);
   if (lane == 0 && cnt) atomicAdd(out, cnt);
-  if (threadIdx.x == 0) mbar_inval(&bar);
+  if (threadIdx.x == 0 && alive) mbar_inval(&bar);
 }
 
 }  // namespace
@@ -799,6 +783,9 @@ int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_o
   if (per_sm < 1) per_sm = 1;
   const unsigned grid = (unsigned)(sm_count() * per_sm);
   const TileRange rng = shard_range(plan->n_cta, plan->n_warp, shard, nshards);
+  const uint32_t words = (uint32_t)(WARPS * kWarpTableSlots);
+  const uint32_t cw = plan->params.cta_set_words;
+  const CtaSetCfg cfg{cw && cw < words ? cw : words, plan->params.stage_polls};
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   GARY_CUDA(cudaStreamIsCapturing(s, &cap));
   const bool timed = cap == cudaStreamCaptureStatusNone;
@@ -806,20 +793,22 @@ int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_o
   GARY_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), s));
   if (timed) GARY_CUDA(cudaEventRecord(g->ev0, s));
   kern<<<grid, WARPS * 32, smem, s>>>(g->view(), plan->in.inedge.p, plan->in.inptr.p, plan->light.p,
-                                      plan->tiles.p, plan->n_cta, rng, plan->sched.p, d_out, ctl);
+                                      plan->tiles.p, plan->n_cta, rng, plan->sched.p, d_out, ctl, cfg);
   GARY_CUDA(cudaGetLastError());
   if (timed) GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
   g->last.tiles = (rng.cta_hi - rng.cta_lo) + (rng.warp_hi - rng.warp_lo);
   g->last.cta_tiles = rng.cta_hi - rng.cta_lo;
+  g->last.work = plan->in.total_work;
   g->last_timed = timed;
+  g->last_sched = plan->sched.p;
   return GARY_OK;
 }
 
 int launch_k3_ctl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
                   uint32_t shard, uint32_t nshards, const uint8_t *variant,
                   unsigned long long *cycles, unsigned long long *gcount) {
-  const VertexCtl ctl{variant, cycles, gcount ? g->gid.p : nullptr, gcount};
+  const VertexCtl ctl{variant, cycles, gcount ? g->gid.p : nullptr, gcount, &plan->sched.p->error};
   if (plan->params.min_blocks >= 3) return launch_k3_impl<3>(g, plan, d_out, s, shard, nshards, ctl);
   return launch_k3_impl<2>(g, plan, d_out, s, shard, nshards, ctl);
 }

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 
+#include "bulk.cuh"
 #include "graph.cuh"
 #include "internal.cuh"
 
@@ -39,12 +40,21 @@ struct Tile {
 // warp_tile_cost and min_blocks left at 0 follow the graph's total work
 // (resolve_params): about 32 warp tiles per resident warp, and 3 resident CTAs
 // per SM once there are 2^31 probes or more.
+//
+// cta_set_words and stage_polls change no plan, only how CTA tiles run; they
+// exist so that tests can reach every CTA set path on small graphs:
+// cta_set_words caps the shared words a CTA tile's set of N+(v) may use (the
+// path is then chosen as if the CTA had only that much shared memory), and
+// stage_polls caps the polls of the first wait for a bulk staging copy (the
+// drain wait after a timeout always keeps the full limit).
 struct PlanParams {
   uint32_t warp_cap = kWarpTableSlots / 2;  // largest d+(v) a warp set takes
   uint64_t warp_tile_cost = 0;              // target probes per warp tile (0: from the work)
   uint64_t cta_tile_cost = 1u << 20;        // target probes per CTA tile
   uint64_t vertex_overhead = 64;            // fixed cost of a middle vertex
   uint32_t min_blocks = 0;                  // resident CTAs per SM, 2 or 3 (0: from the work)
+  uint32_t cta_set_words = 0;               // 0: the CTA's whole shared buffer
+  uint32_t stage_polls = kSpinLimit;        // polls of the first staging wait
 };
 
 // The parameters a plan over `total_work` probes uses: explicit values as
@@ -73,9 +83,13 @@ inline TileRange shard_range(uint32_t n_cta, uint32_t n_warp, uint32_t shard, ui
 struct SchedState {
   uint32_t next_cta;
   uint32_t next_warp;
-  uint32_t error;
+  uint32_t error;     // kLaunchErr* bits
   uint32_t next_aux;  // a third queue (the 4-cycle kernel's medium vertices)
+  uint32_t cta_path[4];  // triangle CTA tiles by the set that held N+(v) (kPath*)
 };
+
+// Sets a triangle CTA tile can hold N+(v) in, cheapest first.
+enum : uint32_t { kPathBitmap = 0, kPathBuckets = 1, kPathStaged = 2, kPathSampled = 3 };
 
 // In-edge index of the middle-vertex formulation.  For every oriented edge
 // u -> v whose list suffix after v is non-empty, and with d+(v) > 0:

@@ -28,30 +28,6 @@ __device__ __forceinline__ int hash_log2(uint32_t items) {
   return l < 5 ? 5 : l;
 }
 
-// Insert distinct keys keys[lo..hi) into an open-addressing table (linear
-// probing).  Every thread of the calling group takes a stride of the keys.
-__device__ __forceinline__ void hash_insert_range(uint32_t *tab, int logT, const uint32_t *keys,
-                                                  uint32_t lo, uint32_t hi, uint32_t tid,
-                                                  uint32_t nthreads) {
-  const uint32_t mask = (1u << logT) - 1, shift = 32 - logT;
-  for (uint32_t i = lo + tid; i < hi; i += nthreads) {
-    uint32_t x = keys[i];
-    uint32_t h = hash_slot(x, shift);
-    while (atomicCAS(&tab[h], kSentinel, x) != kSentinel) h = (h + 1) & mask;
-  }
-}
-
-__device__ __forceinline__ uint32_t hash_contains(const uint32_t *tab, int logT, uint32_t x) {
-  const uint32_t mask = (1u << logT) - 1;
-  uint32_t h = hash_slot(x, 32 - logT);
-  while (true) {
-    uint32_t t = tab[h];
-    if (t == x) return 1;
-    if (t == kSentinel) return 0;
-    h = (h + 1) & mask;
-  }
-}
-
 // Lowest lane index k with incl_k > p, for a non-decreasing per-lane
 // inclusive prefix `incl` (all 32 lanes must call).  5 shuffles.
 __device__ __forceinline__ int warp_owner(uint32_t incl, uint32_t p) {
@@ -170,7 +146,10 @@ struct BitmapSet {
 
 // Bucketised open addressing: 4-slot buckets read with one 16-byte load.
 // Slots of a bucket fill in order, so a bucket with a free last slot ends
-// the probe sequence.
+// the probe sequence.  The builder never fills more than half the slots (it
+// drops keys beyond that and reports kLaunchErrTableFull), so at most half
+// the buckets are full and every probe ends at a bucket with a free last
+// slot: the loop needs no counter (which would cost the hot probe a register).
 struct BucketSet {
   const uint4 *tab;
   uint32_t lo, span, bmask;
@@ -199,7 +178,10 @@ struct SearchSet {
 
 // Builders: `nthreads` threads (a warp or the CTA) cooperate; `sync`
 // separates clear, fill and use.  They need span <= bitmap_max_span(words)
-// (bitmap) or d <= words / 2 (buckets) respectively.
+// (bitmap) or d <= words / 2 (buckets) respectively.  A caller that breaks
+// the bucket rule gets a table of its first words / 2 keys only and
+// kLaunchErrTableFull in *err (when err is not null): a wrong count that is
+// reported, never a probe that cannot end.
 template <typename Sync>
 __device__ __forceinline__ BitmapSet build_bitmap(const uint32_t *__restrict__ av, uint32_t d,
                                                   uint32_t lo, uint32_t span, uint32_t *mem,
@@ -222,25 +204,29 @@ template <typename Sync>
 __device__ __forceinline__ BucketSet build_buckets(const uint32_t *__restrict__ av, uint32_t d,
                                                    uint32_t lo, uint32_t span, uint32_t *mem,
                                                    uint32_t words, uint32_t tid, uint32_t nthreads,
-                                                   Sync sync) {
+                                                   Sync sync, unsigned *err) {
   // buckets = next power of two >= d, at most words / 4
   int lb = d > 1 ? 32 - __clz(d - 1) : 0;
   const int cap = 29 - __clz(words);  // log2(words / 4)
   lb = lb < 3 ? 3 : (lb > cap ? cap : lb);
   const uint32_t nb = 1u << lb;
+  if (d > 2 * nb) {  // more keys than half the slots
+    if (err && tid == 0) atomicOr(err, kLaunchErrTableFull);
+    d = 2 * nb;
+  }
   for (uint32_t i = tid; i < 4 * nb; i += nthreads) mem[i] = kSentinel;
   sync();
   for (uint32_t i = tid; i < d; i += nthreads) {
     const uint32_t x = av[i];
     uint32_t b = (x * kHashMul) >> (32 - lb);
-    while (true) {
+    bool placed = false;
+    for (uint32_t k = 0; k < nb && !placed; ++k) {
       uint32_t *slot = mem + 4 * b;
-      if (atomicCAS(slot, kSentinel, x) == kSentinel) break;
-      if (atomicCAS(slot + 1, kSentinel, x) == kSentinel) break;
-      if (atomicCAS(slot + 2, kSentinel, x) == kSentinel) break;
-      if (atomicCAS(slot + 3, kSentinel, x) == kSentinel) break;
+      placed = atomicCAS(slot, kSentinel, x) == kSentinel || atomicCAS(slot + 1, kSentinel, x) == kSentinel ||
+               atomicCAS(slot + 2, kSentinel, x) == kSentinel || atomicCAS(slot + 3, kSentinel, x) == kSentinel;
       b = (b + 1) & (nb - 1);
     }
+    if (!placed && err) atomicOr(err, kLaunchErrTableFull);
   }
   sync();
   return BucketSet{reinterpret_cast<const uint4 *>(mem), lo, span, nb - 1, 32 - lb};

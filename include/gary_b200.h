@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define GARY_ABI_VERSION 1
+#define GARY_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define GARY_OK 0
@@ -43,6 +43,7 @@ extern "C" {
 #define GARY_ERR_INPUT (-4)       /* malformed graph: unsorted, duplicate, loop, id >= n */
 #define GARY_ERR_TIMEOUT (-5)     /* a bounded device wait expired (scheduler, TMA) */
 #define GARY_ERR_UNSUPPORTED (-6) /* valid request this build cannot serve */
+#define GARY_ERR_INTERNAL (-7)    /* a device table overflowed: a capacity rule was broken */
 
 /* ---- flags for gary_graph_upload / gary_csr_from_edges ----------------- */
 #define GARY_INPUT_SYMMETRIC 0x0u /* CSR lists every undirected edge in both rows */
@@ -136,8 +137,20 @@ int gary_count(gary_graph *g, int pattern, int sched, void *stream, uint64_t *ou
 
 /* Same, asynchronous: the total is written to the device word *d_out (which
  * the call zeroes first, unlike the reference, whose caller must zero it,
- * test/TriQueryTest.cu:117).  No host synchronisation. */
+ * test/TriQueryTest.cu:117).  No host synchronisation.  The launch's own
+ * failures (a bounded wait that expired, a table that overflowed) are only
+ * known once it has run: gary_count_status reports them. */
 int gary_count_async(gary_graph *g, int pattern, int sched, void *stream, uint64_t *d_out);
+
+/* Status of the last counting launch on g (gary_count_async,
+ * gary_count_shard_async, gary_batch_count_async or a replay of a captured
+ * batch): synchronises `stream` (the launch's stream) and returns GARY_OK,
+ * GARY_ERR_TIMEOUT (a bounded device wait expired) or GARY_ERR_INTERNAL (a
+ * shared-memory table overflowed); after either error the count on the
+ * device is incomplete.  gary_count performs this check itself.  The
+ * reference's spins never give up, so it has no counterpart
+ * (include/ops/DeviceQueue.cuh:101-108). */
+int gary_count_status(gary_graph *g, void *stream);
 
 /* One shard of the count: every rank holds the whole graph and counts tile
  * ranges [shard/nshards, (shard+1)/nshards) of the plan; the shard totals sum
@@ -146,15 +159,21 @@ int gary_count_async(gary_graph *g, int pattern, int sched, void *stream, uint64
 int gary_count_shard_async(gary_graph *g, int pattern, int sched, uint32_t shard,
                            uint32_t nshards, void *stream, uint64_t *d_out);
 
-/* Statistics of the last gary_count* on g: kernel time of the counting kernel
- * in milliseconds (CUDA events on its stream; call after that stream is
- * synchronised), tiles, and the variant histogram (hash, search, merge,
- * bitmap).  For benches. */
+/* Statistics of the last gary_count* on g (call after its stream is
+ * synchronised): kernel time of the counting kernel in milliseconds (CUDA
+ * events on its stream), tiles, the triangle kernel's CTA tiles by the
+ * shared-memory set that held N+(v) (bitmap of its id span, hash buckets,
+ * the list staged whole by a bulk copy, evenly spaced samples for the
+ * two-phase search), the launch's error word (0 when it ran clean), and the
+ * triangle plan's work: the ids its kernel probes against a set, summed over
+ * the whole plan (shards included).  For benches and tests. */
 typedef struct gary_count_stats {
   float kernel_ms;
   uint32_t tiles;
   uint32_t cta_tiles;
-  uint32_t variant_tiles[4];
+  uint32_t cta_path_tiles[4];
+  uint32_t error;
+  uint64_t work;
 } gary_count_stats;
 int gary_count_last_stats(gary_graph *g, gary_count_stats *out);
 
@@ -168,9 +187,11 @@ int gary_count_last_stats(gary_graph *g, gary_count_stats *out);
  * scratch is a 128 KiB file-scope device array that every GPU loading the
  * library holds until exit, and n may be at most 33,550,336 vertices (larger
  * n returns GARY_ERR_INVALID).  The first call on a device looks up that
- * array's device address and should come before any stream capture.  All
- * calls share the array, so calls that overlap on the GPU race; each call
- * clears it before use.  Asynchronous on `stream`. */
+ * array's device address and should come before any stream capture; the
+ * address is kept for the life of the process, so after a cudaDeviceReset
+ * (which reloads the module) do not call this entry point again in the same
+ * process.  All calls share the array, so calls that overlap on the GPU race;
+ * each call clears it before use.  Asynchronous on `stream`. */
 int gary_count_triangles_noalloc(const uint64_t *d_indptr, const uint32_t *d_colidx,
                                  const uint32_t *d_deg, uint32_t n, void *stream,
                                  uint64_t *d_out);
@@ -212,6 +233,16 @@ int gary_gen_ba(uint32_t n, uint32_t m, uint64_t seed, uint32_t *src, uint32_t *
  *   "vertex_overhead" fixed cost charged per vertex      (default 64)
  *   "min_blocks"      resident CTAs per SM, 2 or 3; 0 (the default) picks 3
  *                     from 2^31 probes on, else 2
+ *   "warp_cap"        largest out-degree d+(v) a warp's hash set takes
+ *                     (8..512, default 512); larger lists whose id span is
+ *                     too wide for a warp bitmap go to CTA tiles
+ * Two keys change no plan, only how its CTA tiles run, so that small graphs
+ * reach every path (tests use them; production leaves them alone):
+ *   "cta_set_words"   shared words a CTA tile's set of N+(v) may use: a power
+ *                     of two from 64 to 16384, or 0 (the default: all 16384)
+ *   "stage_wait_polls" polls of the first wait for a bulk staging copy
+ *                     (0..2^24, default 2^24); when it gives up the launch
+ *                     reports GARY_ERR_TIMEOUT after draining the copy
  *   "pool_keep_bytes" freed device memory the library keeps for reuse, per
  *                     device and per kind: construction scratch in its
  *                     memory pool across syncs, and the blocks of freed

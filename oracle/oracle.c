@@ -367,3 +367,95 @@ void orc_mlp_grad(const float *params, const float *x, const float *t, const uin
   }
   *loss = L;
 }
+
+/* ---- the synthetic workload (see oracle.h) ------------------------------ */
+
+static uint64_t orc_mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+void orc_gen_rmat(int scale, uint64_t seed, uint64_t first, uint64_t count, uint32_t *src,
+                  uint32_t *dst) {
+  const uint64_t golden = 0x9E3779B97F4A7C15ull;
+  const uint32_t ta = (uint32_t)((57ull << 32) / 100), tb = (uint32_t)((76ull << 32) / 100),
+                 tc = (uint32_t)((95ull << 32) / 100);
+  const uint64_t key = orc_mix64(seed ^ 0x5851F42D4C957F2Dull);
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < (int64_t)count; ++k) {
+    const uint64_t i = first + (uint64_t)k;
+    uint32_t s = 0, d = 0;
+    for (int l = 0; l < scale; l += 2) {
+      const uint64_t r = orc_mix64(key + (i * 16 + (uint64_t)(l >> 1)) * golden);
+      for (int h = 0; h < 2 && l + h < scale; ++h) {
+        const uint32_t x = h ? (uint32_t)(r >> 32) : (uint32_t)r;
+        s = (s << 1) | (uint32_t)(x >= tb);
+        d = (d << 1) | (uint32_t)((x >= ta && x < tb) || x >= tc);
+      }
+    }
+    src[k] = s;
+    dst[k] = d;
+  }
+}
+
+static int cmp_u32(const void *a, const void *b) {
+  const uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+  return (x > y) - (x < y);
+}
+
+int64_t orc_unique_edges(uint32_t n, int64_t m, const uint32_t *src, const uint32_t *dst,
+                         uint32_t *us, uint32_t *vs, int threads) {
+  if (threads > 0) omp_set_num_threads(threads);
+  uint64_t *off = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+  uint64_t *cur = (uint64_t *)malloc(((size_t)n + 1) * sizeof(uint64_t));
+  uint32_t *col = (uint32_t *)malloc((size_t)(m > 0 ? m : 1) * sizeof(uint32_t));
+  uint64_t *keep = (uint64_t *)calloc((size_t)n + 1, sizeof(uint64_t));
+  /* rows by the smaller endpoint */
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < m; ++i) {
+    const uint32_t a = src[i], b = dst[i];
+    if (a == b || a >= n || b >= n) continue;
+    const uint32_t u = a < b ? a : b;
+#pragma omp atomic
+    off[u + 1]++;
+  }
+  for (uint32_t v = 0; v < n; ++v) off[v + 1] += off[v];
+  memcpy(cur, off, ((size_t)n + 1) * sizeof(uint64_t));
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < m; ++i) {
+    const uint32_t a = src[i], b = dst[i];
+    if (a == b || a >= n || b >= n) continue;
+    const uint32_t u = a < b ? a : b, v = a < b ? b : a;
+    uint64_t at;
+#pragma omp atomic capture
+    at = cur[u]++;
+    col[at] = v;
+  }
+  /* sort and dedup every row in place; keep[u + 1] = its unique length */
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t u = 0; u < (int64_t)n; ++u) {
+    uint32_t *r = col + off[u];
+    const uint64_t len = off[u + 1] - off[u];
+    if (len > 1) qsort(r, (size_t)len, sizeof(uint32_t), cmp_u32);
+    uint64_t k = 0;
+    for (uint64_t j = 0; j < len; ++j)
+      if (j == 0 || r[j] != r[j - 1]) r[k++] = r[j];
+    keep[u + 1] = k;
+  }
+  for (uint32_t v = 0; v < n; ++v) keep[v + 1] += keep[v];
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int64_t u = 0; u < (int64_t)n; ++u) {
+    const uint64_t k = keep[u + 1] - keep[u];
+    for (uint64_t j = 0; j < k; ++j) {
+      us[keep[u] + j] = (uint32_t)u;
+      vs[keep[u] + j] = col[off[u] + j];
+    }
+  }
+  const int64_t total = (int64_t)keep[n];
+  free(off);
+  free(cur);
+  free(col);
+  free(keep);
+  return total;
+}

@@ -81,6 +81,23 @@ void orc_mlp_forward(const float *params, const float *x, int64_t n, double *y);
 void orc_mlp_grad(const float *params, const float *x, const float *t, const uint8_t *mask,
                   int64_t n, double norm, double *grad, double *loss);
 
+/* ---- the synthetic workload, restated for the reference arm ------------
+ * bench.py's reference arm must build its input without the product library,
+ * so the seeded RMAT generator (a workload definition of this project, not a
+ * reference algorithm) is restated here: counter-based splitmix64 draws,
+ * (a,b,c,d) = (.57,.19,.19,.05) by integer thresholds floor(2^32 *
+ * {.57,.76,.95}), two levels per 64-bit draw, no noise, no permutation.
+ * tests/test_oracle.py checks it edge for edge against gary_gen_rmat. */
+void orc_gen_rmat(int scale, uint64_t seed, uint64_t first, uint64_t count, uint32_t *src,
+                  uint32_t *dst);
+
+/* Unique undirected edges of an edge list over [0, n): self loops dropped,
+ * duplicates in either direction merged, each edge written once as
+ * (us[k], vs[k]) with us[k] < vs[k], sorted by (u, v).  us and vs hold m
+ * entries.  Returns the number written.  OpenMP over rows. */
+int64_t orc_unique_edges(uint32_t n, int64_t m, const uint32_t *src, const uint32_t *dst,
+                         uint32_t *us, uint32_t *vs, int threads);
+
 #ifdef __cplusplus
 }
 #endif

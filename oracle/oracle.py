@@ -37,6 +37,8 @@ _ORC = {
     "orc_build_cache": (None, [_P, _I64, _INT, _P]),
     "orc_binary_search_2phase": (_INT, [_P, _I64, _P, _INT, _U32]),
     "orc_mlp_forward": (None, [_P, _P, _I64, _P]),
+    "orc_gen_rmat": (None, [_INT, _U64, _U64, _U64, _P, _P]),
+    "orc_unique_edges": (_I64, [_U32, _I64, _P, _P, _P, _P, _INT]),
     "orc_mlp_grad": (None, [_P, _P, _P, _P, _I64, C.c_double, _P, C.POINTER(C.c_double)]),
 }
 
@@ -188,6 +190,24 @@ def binary_search_2phase(lst, keys, N: int = 32) -> np.ndarray:
         [orc().orc_binary_search_2phase(lst.ctypes.data, len(lst), c.ctypes.data, N, int(k)) for k in keys],
         np.uint8,
     )
+
+
+def gen_rmat(scale: int, seed: int, count: int, first: int = 0):
+    """The seeded RMAT workload's edges, restated (no product library)."""
+    src = np.empty(count, np.uint32)
+    dst = np.empty(count, np.uint32)
+    orc().orc_gen_rmat(scale, seed, first, count, src.ctypes.data, dst.ctypes.data)
+    return src, dst
+
+
+def unique_edges(n: int, src, dst, threads: int = 0):
+    """Each undirected edge once, (u < v), loops dropped, sorted by (u, v)."""
+    src, dst = _a(src, np.uint32), _a(dst, np.uint32)
+    us = np.empty(max(len(src), 1), np.uint32)
+    vs = np.empty(max(len(src), 1), np.uint32)
+    k = orc().orc_unique_edges(n, len(src), src.ctypes.data, dst.ctypes.data, us.ctypes.data, vs.ctypes.data,
+                               threads)
+    return us[:k], vs[:k]
 
 
 def unique_pairs(sym_ptr, sym_idx) -> tuple[np.ndarray, np.ndarray]:

@@ -71,3 +71,49 @@ def test_batched_counts_match_per_graph_and_oracle(cuda):
         assert int(exe.total.item()) == total
     exe.free()
     batch.free()
+
+
+@pytest.mark.gpu
+def test_full_4096_graph_batch(cuda):
+    """The batched workload at its full size: 4096 graphs, n log-uniform in
+    [1e3, 2e5], half Barabasi-Albert (m in 2..16), half RMAT ef8, counted in
+    one launch.  Every graph's count equals its own upload counted alone, and
+    a spread of graphs (the smallest, the largest, every 256th) equals the CPU
+    oracle."""
+    import ctypes as C
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    import gary_b200 as gb
+    from gary_b200 import _lib
+
+    specs = B.make_specs(4096, seed=1)
+    batch = B.Batch.build(specs)
+    try:
+        counts, total = batch.count()
+        st = batch.graph.status()
+        assert st == 0
+    finally:
+        batch.free()
+    torch.cuda.empty_cache()
+    assert total == int(counts.sum())
+    ns = np.array([s.n for s in specs])
+    sample = sorted({int(ns.argmin()), int(ns.argmax()), *range(0, 4096, 256), *range(1, 4096, 256)})
+    with ThreadPoolExecutor(16) as ex:
+        for lo in range(0, 4096, 512):
+            edges = list(ex.map(B.generate, specs[lo:lo + 512]))
+            for k, (s, d) in enumerate(edges):
+                spec = specs[lo + k]
+                with gb.csr_from_edges_device(s, d, spec.n) as csr:
+                    p, i = csr.device_ptrs()
+                    _, nnz = csr.shape()
+                    h = C.c_void_p()
+                    _lib.check(_lib.load().gary_graph_upload(p, i, spec.n, nnz, _lib.GARY_INPUT_DEVICE, None,
+                                                             C.byref(h)), "upload")
+                with gb.Graph(h.value) as g:
+                    assert g.count() == int(counts[spec.index]), spec
+                if spec.index in sample:
+                    ptr, idx = O.sym_csr(s, d, spec.n)
+                    dp, di = O.orient(ptr, idx)
+                    assert O.tri_count(dp, di) == int(counts[spec.index]), spec

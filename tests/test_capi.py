@@ -33,7 +33,7 @@ def test_every_declared_symbol_is_exported():
 
 
 def test_abi_version():
-    assert _lib.load().gary_abi_version() == 1
+    assert _lib.load().gary_abi_version() == 2
 
 
 def test_argument_errors_without_device():
@@ -80,7 +80,27 @@ def test_header_compiles_as_c():
 
     with tempfile.TemporaryDirectory() as d:
         src = Path(d) / "t.c"
-        src.write_text('#include "gary_b200.h"\nint main(void){return gary_abi_version() != 1;}\n')
+        src.write_text('#include "gary_b200.h"\nint main(void){return gary_abi_version() != 2;}\n')
         r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", f"-I{ROOT / 'include'}", "-c", str(src),
                             "-o", str(Path(d) / "t.o")], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
+
+
+def test_tuning_keys_checked():
+    """gary_tune validates every key's range on the host (no device needed)."""
+    L = _lib.load()
+    try:
+        for key, bad in (("warp_cap", 4), ("warp_cap", 1024), ("cta_set_words", 100), ("cta_set_words", 32),
+                         ("cta_set_words", 32768), ("stage_wait_polls", (1 << 24) + 1), ("min_blocks", 1),
+                         ("no_such_key", 1)):
+            assert L.gary_tune(key.encode(), bad) == _lib.GARY_ERR_INVALID, (key, bad)
+        for key, good in (("warp_cap", 8), ("cta_set_words", 64), ("cta_set_words", 0),
+                          ("stage_wait_polls", 0), ("min_blocks", 3)):
+            assert L.gary_tune(key.encode(), good) == _lib.GARY_OK, (key, good)
+    finally:
+        assert L.gary_tune(b"reset", 0) == _lib.GARY_OK
+
+
+def test_count_status_needs_a_launch():
+    L = _lib.load()
+    assert L.gary_count_status(None, None) == _lib.GARY_ERR_INVALID

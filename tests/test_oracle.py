@@ -184,3 +184,30 @@ def test_er_generator():
     assert len(np.unique(keys)) == 20000
     s2, d2 = gb.gen_er(1000, 20000, 4)
     assert np.array_equal(s, s2) and np.array_equal(d, d2)
+
+
+@pytest.mark.parametrize("scale,seed,first,count", [(12, 3, 0, 1 << 16), (24, 1, 12_345_678, 100_000),
+                                                    (31, 9, 0, 1000), (1, 2, 0, 50), (17, 4, 7, 3)])
+def test_rmat_restatement_matches_library(scale, seed, first, count):
+    """The oracle's RMAT restatement (used by bench.py's reference arm, which
+    must not load the product library) is the library's generator, edge for
+    edge (gary_gen_rmat runs on the host)."""
+    import gary_b200 as gb
+
+    a_src, a_dst = gb.gen_rmat(scale, seed, count, first)
+    b_src, b_dst = O.gen_rmat(scale, seed, count, first)
+    assert np.array_equal(a_src, b_src) and np.array_equal(a_dst, b_dst)
+
+
+def test_unique_edges_match_symmetric_csr():
+    """orc_unique_edges (each undirected edge once, loops dropped) is the
+    edge set of the oracle's symmetric CSR, in the same (u, v) order."""
+    for scale, ef, seed in ((10, 16, 1), (14, 8, 4)):
+        n = 1 << scale
+        s, d = O.gen_rmat(scale, seed, ef << scale)
+        s = np.concatenate([s, d[:100], np.arange(50, dtype=np.uint32)])  # reversed duplicates, loops
+        d = np.concatenate([d, s[:100], np.arange(50, dtype=np.uint32)])
+        us, vs = O.unique_edges(n, s, d)
+        pu, pv = O.unique_pairs(*O.sym_csr(s, d, n))
+        assert np.array_equal(us, pu) and np.array_equal(vs, pv)
+        assert np.all(us < vs)
