@@ -71,6 +71,8 @@ def parse():
                     help="tc: the headline triangle count; setops: the set-intersection microbench; "
                          "batch: 4096 graphs in one launch; patterns: triangle / 4-cycle / 4-clique "
                          "counts on the RMAT graph")
+    ap.add_argument("--cpu-scale", type=int, default=16,
+                    help="patterns: RMAT scale of the graph the CPU oracle counts beside the GPU")
     ap.add_argument("--patterns", default="3,4,5",
                     help="patterns workload: 3 triangle, 4 four-cycle, 5 four-clique")
     ap.add_argument("--graphs", type=int, default=4096, help="batch: number of graphs")
@@ -78,6 +80,9 @@ def parse():
     ap.add_argument("--pairs-log2", type=int, default=24, help="setops: total pairs = 2^k")
     ap.add_argument("--batch-log2", type=int, default=20, help="setops: pairs per generated batch")
     ap.add_argument("--overlaps", default="0,0.1,0.25,0.5", help="setops: planted overlap fractions")
+    ap.add_argument("--src-block-mb", type=float, default=None,
+                    help="MB of lists per source block of the triangle plan (0: the library's "
+                         "default; negative: one block, i.e. no blocking)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-schedule leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batch and set-intersection summaries of the default line")
@@ -363,6 +368,9 @@ def run_ours(args, dist):
     dev = dist.local
     if args.pool_keep_gb is not None:
         _lib.check(_lib.load().gary_tune(b"pool_keep_bytes", int(args.pool_keep_gb * 1e9)), "gary_tune")
+    if args.src_block_mb is not None:
+        blk = 1 << 62 if args.src_block_mb < 0 else int(args.src_block_mb * (1 << 20)) // 32 * 32
+        _lib.check(_lib.load().gary_tune(b"src_block_bytes", blk), "gary_tune")
     sched = {"plain": _lib.GARY_SCHED_PLAIN, "learned": _lib.GARY_SCHED_LEARNED}[args.sched]
     if args.sched == "learned" or not args.no_learned:
         from gary_b200.costmodel import CostModel
@@ -392,11 +400,13 @@ def run_ours(args, dist):
     if not args.no_learned:
         other = _lib.GARY_SCHED_PLAIN if args.sched == "learned" else _lib.GARY_SCHED_LEARNED
         lper, lcount, _ = time_counts(L, g, other, dist, stream, out, args.steps, args.warmup)
+        lstats = g.last_stats()
         lms = dist.allreduce(sum(lper) / len(lper), "max")
         lcount = dist.allreduce(lcount, "sum")
         learned_ms, plain_ms = (lms, ms) if other == _lib.GARY_SCHED_LEARNED else (ms, lms)
         learned = {"value": m / (learned_ms / 1e3), "unit": UNIT, "ms": learned_ms, "plain_ms": plain_ms,
                    "ratio_vs_plain": plain_ms / learned_ms, "count_equal": lcount == count,
+                   "balance": balance_of(lstats),
                    "model": "gary_b200/data/cost_model.gmlp (6-64-64-4 MLP, per-vertex variant and tile weights)"}
         assert lcount == count, f"learned schedule count {lcount} != plain {count}"
 
@@ -498,6 +508,11 @@ def run_ours(args, dist):
             "clocks": clk,
             "build_s": build_s,
             "cta_path_tiles": stats.get("cta_path_tiles"),
+            "src_block": ("library default (48 MB of lists per block)" if args.src_block_mb in (None, 0)
+                          else "one block" if args.src_block_mb < 0 else f"{args.src_block_mb} MB"),
+            # the last timed launch's makespan against the mean CTA finish: how much any other
+            # assignment of the same tiles to CTAs could gain
+            "balance": balance_of(stats),
         }
     g_dag = None
     if dist.rank == 0 and dist.world == 1 and not args.no_ref_gpu:
@@ -542,6 +557,11 @@ def run_ours(args, dist):
         print(json.dumps(line), flush=True)
     dist.close()
     return 0
+
+
+def balance_of(stats: dict) -> dict:
+    mk, mean = stats.get("makespan_ms") or 0.0, stats.get("mean_cta_finish_ms") or 0.0
+    return {"makespan_ms": mk, "mean_cta_finish_ms": mean, "schedule_bound": mk / mean if mean else None}
 
 
 def sm_count() -> int:
@@ -790,39 +810,71 @@ def run_patterns(args, dist):
     """Triangle, 4-cycle and 4-clique counts of the seeded RMAT graph (one GPU):
     per pattern the first call (plan building included, wall clock) and the
     mean of `steps` counts after `warmup` (CUDA events on the counting stream,
-    plan cached).  One JSON line per pattern."""
+    plan cached).  Beside it, the same pattern on RMAT scale --cpu-scale
+    (default 16) counted by the GPU and by the CPU oracle (all host threads),
+    with equal counts: the oracle cannot count the full graph in reasonable
+    time.  One JSON line per pattern."""
+    import numpy as np
     import torch
 
     import gary_b200 as gb
-    from gary_b200 import _lib
+    from oracle import oracle as O  # the small-graph CPU baseline only
 
     torch.cuda.set_device(dist.local)
     n, csr = build_graph(gb, torch, args.scale, args.ef, args.seed)
     g = upload_from_device_csr(gb, csr, n)
     csr.free()
+    m = g.info()["m"]
+    # the small graph for the CPU comparison
+    sn = 1 << args.cpu_scale
+    ss, sd = gb.gen_rmat(args.cpu_scale, args.seed, args.ef << args.cpu_scale)
+    sptr, sidx = gb.csr_from_edges(ss, sd, sn)
+    dptr, didx = O.orient(sptr, sidx)
+    small = gb.Graph.upload(sptr, sidx, sn)
     stream = torch.cuda.Stream()
     out = torch.zeros(1, dtype=torch.int64, device="cuda")
     names = {3: "triangle", 4: "4-cycle", 5: "4-clique"}
+
+    def timed(graph, pat, steps):
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                graph.count_async(out, pat, stream=stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                graph.count_async(out, pat, stream=stream)
+            e1.record(stream)
+        stream.synchronize()
+        graph.check_status(stream)
+        return e0.elapsed_time(e1) / max(steps, 1), int(out.item())
+
     for pat in (int(x) for x in args.patterns.split(",")):
         with torch.cuda.stream(stream):
             t0 = time.perf_counter()
             g.count_async(out, pat, stream=stream)
             stream.synchronize()
             first_s = time.perf_counter() - t0
-            for _ in range(args.warmup):
-                g.count_async(out, pat, stream=stream)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(args.steps):
-                g.count_async(out, pat, stream=stream)
-            e1.record(stream)
-        stream.synchronize()
-        ms = e0.elapsed_time(e1) / max(args.steps, 1)
+        ms, cnt = timed(g, pat, args.steps)
+        sms, scnt = timed(small, pat, max(args.steps, 5))
+        oracle = {3: lambda: O.tri_count(dptr, didx), 4: lambda: O.c4_count(sptr, sidx),
+                  5: lambda: O.k4_count(dptr, didx)}[pat]
+        t0 = time.perf_counter()
+        ocnt = oracle()
+        cpu_s = time.perf_counter() - t0
+        assert ocnt == scnt, f"{names[pat]}: oracle {ocnt} != GPU {scnt} on the small graph"
         print(json.dumps({"metric": f"{names[pat]} count time", "value": ms, "unit": "ms", "higher_is_better": False,
-                          "pattern": names[pat], "count": int(out.item()), "first_call_s": first_s,
+                          "pattern": names[pat], "count": cnt, "first_call_s": first_s,
+                          "oriented_edges_per_s": m / (ms / 1e3),
                           "steps": args.steps, "warmup": args.warmup, "n_gpus": 1, "data": "synthetic",
                           "config": {"workload": f"{names[pat]} count, RMAT scale {args.scale} edge factor "
-                                                 f"{args.ef}, seed {args.seed}"}}), flush=True)
+                                                 f"{args.ef}, seed {args.seed}"},
+                          "small_graph": {"workload": f"RMAT scale {args.cpu_scale} edge factor {args.ef}",
+                                          "gpu_ms": sms, "count": scnt,
+                                          "cpu_baseline": {"value": cpu_s * 1e3, "unit": "ms", "kind": "port",
+                                                           "cores": os.cpu_count(),
+                                                           "sample": "the whole small graph, CPU oracle"},
+                                          "gpu_vs_cpu": cpu_s * 1e3 / sms}}), flush=True)
+    small.free()
     g.free()
     return 0
 

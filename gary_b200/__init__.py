@@ -172,7 +172,8 @@ class Graph:
         check(load().gary_count_last_stats(self._h, C.byref(st)), "gary_count_last_stats")
         return {"kernel_ms": st.kernel_ms, "tiles": st.tiles, "cta_tiles": st.cta_tiles,
                 "cta_path_tiles": dict(zip(("bitmap", "buckets", "staged", "sampled"), st.cta_path_tiles)),
-                "error": st.error, "work": st.work}
+                "error": st.error, "work": st.work, "makespan_ms": st.makespan_ms,
+                "mean_cta_finish_ms": st.mean_cta_finish_ms}
 
 
 class DeviceCsr:

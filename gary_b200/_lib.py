@@ -83,6 +83,8 @@ class CountStats(C.Structure):
         ("cta_path_tiles", C.c_uint32 * 4),  # bitmap, buckets, staged whole, sampled
         ("error", C.c_uint32),
         ("work", C.c_uint64),
+        ("makespan_ms", C.c_float),
+        ("mean_cta_finish_ms", C.c_float),
     ]
 
 

@@ -2,6 +2,7 @@
 // No C++ exception crosses this boundary: every entry point catches and maps
 // to a GARY_ERR_* status (the reference's checkCudaErrors exits the process
 // instead, common/HelperCUDA.h:582-595).
+#include <algorithm>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -368,6 +369,8 @@ extern "C" int gary_tune(const char *key, uint64_t value) {
   else if (k == "cta_set_words" && (value == 0 || (pow2 && value >= 64 && value <= gary::kTcWarps * gary::kWarpTableSlots)))
     p.cta_set_words = (uint32_t)value;
   else if (k == "stage_wait_polls" && value <= gary::kSpinLimit) p.stage_polls = (uint32_t)value;
+  else if (k == "src_block_bytes" && (value == 0 || (value >= (1u << 20) && value % 32 == 0)))
+    p.src_block_words = value / 4;
   else if (k == "vertex_overhead") p.vertex_overhead = value;
   else if (k == "min_blocks" && (value == 0 || value == 2 || value == 3)) p.min_blocks = (uint32_t)value;
   else if (k == "pool_keep_bytes") gary::set_pool_keep_bytes(value);
@@ -634,6 +637,21 @@ extern "C" int gary_count_last_stats(gary_graph *g, gary_count_stats *out) {
     GARY_CUDA(cudaMemcpy(&st, g->last_sched, sizeof(st), cudaMemcpyDeviceToHost));
     for (int k = 0; k < 4; ++k) g->last.cta_path_tiles[k] = st.cta_path[k];
     g->last.error = st.error;
+  }
+  if (g->last_span && g->last_span_ctas) {
+    // makespan of the launch and the mean time at which its CTAs finished,
+    // both from the earliest CTA start
+    std::vector<unsigned long long> sp(2ull * g->last_span_ctas);
+    GARY_CUDA(cudaMemcpy(sp.data(), g->last_span, sp.size() * 8, cudaMemcpyDeviceToHost));
+    unsigned long long t0 = ~0ull, t1 = 0;
+    for (uint32_t b = 0; b < g->last_span_ctas; ++b) {
+      t0 = std::min(t0, sp[2 * b]);
+      t1 = std::max(t1, sp[2 * b + 1]);
+    }
+    double mean = 0;
+    for (uint32_t b = 0; b < g->last_span_ctas; ++b) mean += (double)(sp[2 * b + 1] - t0);
+    g->last.makespan_ms = (float)((t1 - t0) * 1e-6);
+    g->last.mean_cta_finish_ms = (float)(mean / g->last_span_ctas * 1e-6);
   }
   if (g->last_timed) {
     float ms = 0.f;

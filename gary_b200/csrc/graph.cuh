@@ -75,6 +75,8 @@ struct gary_graph {
   gary_count_stats last{};
   bool last_timed = false;  // ev0/ev1 bracket the last counting kernel
   const gary::SchedState *last_sched = nullptr;  // scheduler words of the last counting launch
+  const unsigned long long *last_span = nullptr;   // triangle launches: per-CTA start / finish ns
+  uint32_t last_span_ctas = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   gary::GraphView view() const { return gary::GraphView{n, dag.row.p, dag.adj.p, true}; }

@@ -914,6 +914,7 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   g->last.cta_tiles = (b1 - b0) + (m1 - m0);
   g->last_timed = true;
   g->last_sched = st;
+  g->last_span = nullptr;
   return GARY_OK;
 }
 
@@ -1040,6 +1041,7 @@ int launch_c4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   g->last.cta_tiles = (t1 - t0) + (m1 - m0);
   g->last_timed = true;
   g->last_sched = plan->sched.p;
+  g->last_span = nullptr;
   return GARY_OK;
 }
 

@@ -166,7 +166,10 @@ int gary_count_shard_async(gary_graph *g, int pattern, int sched, uint32_t shard
  * the list staged whole by a bulk copy, evenly spaced samples for the
  * two-phase search), the launch's error word (0 when it ran clean), and the
  * triangle plan's work: the ids its kernel probes against a set, summed over
- * the whole plan (shards included).  For benches and tests. */
+ * the whole plan (shards included).  For the triangle kernel also its makespan
+ * and the mean time at which its CTAs finished (device clock, from the first
+ * CTA start): makespan / mean finish bounds what any other assignment of the
+ * same tiles to CTAs could gain.  For benches and tests. */
 typedef struct gary_count_stats {
   float kernel_ms;
   uint32_t tiles;
@@ -174,6 +177,8 @@ typedef struct gary_count_stats {
   uint32_t cta_path_tiles[4];
   uint32_t error;
   uint64_t work;
+  float makespan_ms;
+  float mean_cta_finish_ms;
 } gary_count_stats;
 int gary_count_last_stats(gary_graph *g, gary_count_stats *out);
 
@@ -233,6 +238,11 @@ int gary_gen_ba(uint32_t n, uint32_t m, uint64_t seed, uint32_t *src, uint32_t *
  *   "vertex_overhead" fixed cost charged per vertex      (default 64)
  *   "min_blocks"      resident CTAs per SM, 2 or 3; 0 (the default) picks 3
  *                     from 2^31 probes on, else 2
+ *   "src_block_bytes" bytes of adjacency per source block of the triangle plan
+ *                     (the kernel runs the blocks one after another so that the
+ *                     lists one block reads stay in L2); 0 (the default) takes
+ *                     48 MB, and one block when the lists fit in 96 MB; else at
+ *                     least 2^20 and a multiple of 32
  *   "warp_cap"        largest out-degree d+(v) a warp's hash set takes
  *                     (8..512, default 512); larger lists whose id span is
  *                     too wide for a warp bitmap go to CTA tiles
