@@ -80,9 +80,6 @@ def parse():
     ap.add_argument("--pairs-log2", type=int, default=24, help="setops: total pairs = 2^k")
     ap.add_argument("--batch-log2", type=int, default=20, help="setops: pairs per generated batch")
     ap.add_argument("--overlaps", default="0,0.1,0.25,0.5", help="setops: planted overlap fractions")
-    ap.add_argument("--src-block-mb", type=float, default=None,
-                    help="MB of lists per source block of the triangle plan (0: the library's "
-                         "default; negative: one block, i.e. no blocking)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-schedule leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batch and set-intersection summaries of the default line")
@@ -368,9 +365,6 @@ def run_ours(args, dist):
     dev = dist.local
     if args.pool_keep_gb is not None:
         _lib.check(_lib.load().gary_tune(b"pool_keep_bytes", int(args.pool_keep_gb * 1e9)), "gary_tune")
-    if args.src_block_mb is not None:
-        blk = 1 << 62 if args.src_block_mb < 0 else int(args.src_block_mb * (1 << 20)) // 32 * 32
-        _lib.check(_lib.load().gary_tune(b"src_block_bytes", blk), "gary_tune")
     sched = {"plain": _lib.GARY_SCHED_PLAIN, "learned": _lib.GARY_SCHED_LEARNED}[args.sched]
     if args.sched == "learned" or not args.no_learned:
         from gary_b200.costmodel import CostModel
@@ -508,8 +502,6 @@ def run_ours(args, dist):
             "clocks": clk,
             "build_s": build_s,
             "cta_path_tiles": stats.get("cta_path_tiles"),
-            "src_block": ("library default (48 MB of lists per block)" if args.src_block_mb in (None, 0)
-                          else "one block" if args.src_block_mb < 0 else f"{args.src_block_mb} MB"),
             # the last timed launch's makespan against the mean CTA finish: how much any other
             # assignment of the same tiles to CTAs could gain
             "balance": balance_of(stats),

@@ -369,8 +369,6 @@ extern "C" int gary_tune(const char *key, uint64_t value) {
   else if (k == "cta_set_words" && (value == 0 || (pow2 && value >= 64 && value <= gary::kTcWarps * gary::kWarpTableSlots)))
     p.cta_set_words = (uint32_t)value;
   else if (k == "stage_wait_polls" && value <= gary::kSpinLimit) p.stage_polls = (uint32_t)value;
-  else if (k == "src_block_bytes" && (value == 0 || (value >= (1u << 20) && value % 32 == 0)))
-    p.src_block_words = value / 4;
   else if (k == "vertex_overhead") p.vertex_overhead = value;
   else if (k == "min_blocks" && (value == 0 || value == 2 || value == 3)) p.min_blocks = (uint32_t)value;
   else if (k == "pool_keep_bytes") gary::set_pool_keep_bytes(value);

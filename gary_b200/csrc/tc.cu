@@ -19,7 +19,6 @@
 // Work is cut into tiles of bounded probe count over the in-edge index and
 // served by a persistent scheduler: CTA tiles (large N+(v)) first, then warp
 // tiles.
-#include <cub/cub.cuh>
 #include <thrust/binary_search.h>
 #include <thrust/copy.h>
 #include <thrust/execution_policy.h>
@@ -28,12 +27,10 @@
 #include <thrust/iterator/transform_iterator.h>
 #include <thrust/reduce.h>
 #include <thrust/scan.h>
-#include <thrust/sequence.h>
 #include <thrust/transform.h>
 
 #include <algorithm>
 #include <memory>
-#include <vector>
 
 #include "bulk.cuh"
 #include "mlp.cuh"
@@ -69,12 +66,12 @@ __host__ __device__ __forceinline__ uint64_t min_u64(uint64_t a, uint64_t b) { r
 // does not depend on it.
 template <typename F>
 __device__ __forceinline__ void walk_records(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
-                                             uint32_t u0, uint32_t u1, F f) {
+                                             uint32_t n, F f) {
   const int lane = threadIdx.x & 31;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; u0 + c * 32 < u1; c += nwarps) {
-    const uint64_t u = u0 + c * 32 + lane;
-    const uint2 r = u < u1 ? row[u] : make_uint2(0, 0);
+  for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c * 32 < n; c += nwarps) {
+    const uint64_t u = c * 32 + lane;
+    const uint2 r = u < n ? row[u] : make_uint2(0, 0);
     const uint32_t incl = warp_inclusive_sum(r.y, lane);
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     for (uint32_t pb = 0; pb < total; pb += 32) {
@@ -94,164 +91,88 @@ __device__ __forceinline__ void walk_records(const uint2 *__restrict__ row, cons
   }
 }
 
-// Rows [u0, u1) form one source block: launched block after block, the
-// count hands out slots in block order, so each vertex's records come out
-// grouped by source block.
-__global__ void k_in_count(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj, uint32_t u0,
-                           uint32_t u1, uint32_t *__restrict__ cnt, unsigned long long *__restrict__ work,
+__global__ void k_in_count(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj, uint32_t n,
+                           uint32_t *__restrict__ cnt, unsigned long long *__restrict__ work,
                            uint32_t *__restrict__ slot) {
-  walk_records(row, adj, u0, u1, [&](uint64_t w, uint32_t v, uint32_t rem) {
+  walk_records(row, adj, n, [&](uint64_t w, uint32_t v, uint32_t rem) {
     slot[w] = atomicAdd(&cnt[v], 1u);
     atomicAdd(&work[v], (unsigned long long)rem);
   });
 }
 
-// recvp[k] = {v, source block} of record k (plan scratch).
-__global__ void k_in_fill(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj, uint32_t u0,
-                          uint32_t u1, uint32_t blk, const uint64_t *__restrict__ inptr,
-                          const uint32_t *__restrict__ slot, uint2 *__restrict__ inedge,
-                          uint2 *__restrict__ recvp) {
-  walk_records(row, adj, u0, u1, [&](uint64_t w, uint32_t v, uint32_t rem) {
-    const uint64_t k = inptr[v] + slot[w];
-    inedge[k] = make_uint2((uint32_t)(w + 1), rem);
-    recvp[k] = make_uint2(v, blk);
+__global__ void k_in_fill(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj, uint32_t n,
+                          const uint64_t *__restrict__ inptr, const uint32_t *__restrict__ slot,
+                          uint2 *__restrict__ inedge) {
+  walk_records(row, adj, n, [&](uint64_t w, uint32_t v, uint32_t rem) {
+    inedge[inptr[v] + slot[w]] = make_uint2((uint32_t)(w + 1), rem);
   });
-}
-
-// ublk[p] = first row whose list starts at or after word p * bw (ublk[P] = n):
-// rows [ublk[p], ublk[p+1]) form source block p.
-__global__ void k_block_rows(const uint2 *__restrict__ row, uint32_t n, uint64_t bw, uint32_t P,
-                             uint32_t *__restrict__ ublk) {
-  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p <= P;
-       p += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t b = 0, e = n;
-    const uint64_t target = p * bw;
-    while (b < e) {
-      const uint32_t m = (b + e) >> 1;
-      if ((uint64_t)row[m].x * 4 < target) b = m + 1;
-      else e = m;
-    }
-    ublk[p] = p == P ? n : b;
-  }
-}
-
-// ---- pieces: the records of one middle vertex from one source block --------
-__global__ void k_piece_heads(const uint2 *__restrict__ recvp, uint64_t m, uint32_t *__restrict__ head) {
-  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k <= m;
-       k += (uint64_t)gridDim.x * blockDim.x) {
-    uint32_t h = 0;
-    if (k < m) {
-      const uint2 t = recvp[k];
-      h = k == 0 || t.x != recvp[k - 1].x || t.y != recvp[k - 1].y;
-    }
-    head[k] = h;
-  }
-}
-
-// pid[k] = piece of record k (exclusive scan of the heads).  Writes each
-// piece's vertex, block and first record (relative to the vertex), and its
-// work (sum of suffix lengths; a segmented warp sum, one atomic per run).
-__global__ void k_piece_fill(const uint2 *__restrict__ recvp, const uint2 *__restrict__ inedge,
-                             const uint64_t *__restrict__ inptr, uint64_t m, const uint32_t *__restrict__ pid,
-                             uint32_t *__restrict__ pv, uint32_t *__restrict__ pblk, uint32_t *__restrict__ pj0,
-                             unsigned long long *__restrict__ pwork) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < m; base += stride) {
-    const uint64_t k = base + threadIdx.x;
-    const bool ok = k < m;
-    const uint32_t id = ok ? pid[k] : 0xFFFFFFFFu;
-    unsigned long long x = 0;
-    if (ok) {
-      const uint2 t = recvp[k];
-      x = inedge[k].y;
-      if (k == 0 || t.x != recvp[k - 1].x || t.y != recvp[k - 1].y) {
-        pv[id] = t.x;
-        pblk[id] = t.y;
-        pj0[id] = (uint32_t)(k - inptr[t.x]);
-      }
-    }
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned long long y = __shfl_up_sync(kFull, x, o);
-      const uint32_t yi = __shfl_up_sync(kFull, id, o);
-      if (lane >= o && yi == id) x += y;
-    }
-    const uint32_t nid = __shfl_down_sync(kFull, id, 1);
-    if (ok && (lane == 31 || nid != id) && x) atomicAdd(&pwork[id], x);
-  }
 }
 
 struct U32ToU64 {
   __host__ __device__ uint64_t operator()(uint32_t x) const { return x; }
 };
 
-// Per piece, in block order (q = order[i]): its record range [j0, j1), the
-// tiles it needs and, for a light piece, its cost.  A vertex whose N+(v)
-// fits no warp set takes CTA tiles; the others split into warp tiles when
-// their cost passes the tile target and join group tiles otherwise.
-// pcost (learned plans): predicted cycles of a warp-class vertex, shared out
-// over its pieces by work, with tile target tw in the same unit; without it,
-// costs are probe counts.
-__global__ void k_classify_pieces(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
-                                  const uint64_t *__restrict__ inptr, const uint64_t *__restrict__ work,
-                                  const uint32_t *__restrict__ order, uint32_t np,
-                                  const uint32_t *__restrict__ pv, const uint32_t *__restrict__ pblk,
-                                  const uint32_t *__restrict__ pj0, const unsigned long long *__restrict__ pwork,
-                                  PlanParams pp, const uint64_t *__restrict__ pcost, uint64_t tw,
-                                  uint3 *__restrict__ spiece, uint32_t *__restrict__ sblk,
-                                  uint32_t *__restrict__ kC, uint32_t *__restrict__ kW,
-                                  uint64_t *__restrict__ lcost) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < np;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t q = order[i];
-    const uint32_t v = pv[q];
-    const uint32_t nin = (uint32_t)(inptr[v + 1] - inptr[v]);
-    const uint32_t j0 = pj0[q];
-    const uint32_t j1 = q + 1 < np && pv[q + 1] == v ? pj0[q + 1] : nin;
+// pcost (optional): predicted cycles of a warp-class vertex, with tile target
+// tw_pred in the same unit; without it, costs are probe counts.
+__global__ void k_classify(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
+                           const uint64_t *__restrict__ work,
+                           const uint64_t *__restrict__ inptr, uint32_t n, PlanParams pp,
+                           const uint64_t *__restrict__ pcost, uint64_t tw_pred,
+                           uint8_t *__restrict__ vclass, uint64_t *__restrict__ costL,
+                           uint32_t *__restrict__ kW, uint32_t *__restrict__ kC) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
     const uint2 rv = row[v];
     const uint32_t dv = rv.y;
-    // a warp holds N+(v) as a bitmap when its id span is short, else as
-    // buckets when d+(v) <= warp_cap; otherwise the CTA shares one set
-    const uint32_t span = adj[(uint64_t)rv.x * 4 + dv - 1] - adj[(uint64_t)rv.x * 4];
-    const bool bitmap = span <= bitmap_max_span(kWarpTableSlots);
-    const bool warp_fits = bitmap || dv <= pp.warp_cap;
-    const uint64_t build = bitmap ? (span >> 5) + dv : 4ull * dv;
-    const uint64_t pw = pwork[q];
-    const bool pred = pcost && warp_fits;
-    const uint64_t c = pred ? pcost[v] * pw / (work[v] ? work[v] : 1) + 1 : pw + build + pp.vertex_overhead;
-    uint32_t kc = 0, kw = 0;
-    uint64_t lc = 0;
-    if (!warp_fits) kc = (uint32_t)min_u64((c + pp.cta_tile_cost - 1) / pp.cta_tile_cost, j1 - j0);
-    else if (c > tw) kw = (uint32_t)min_u64((c + tw - 1) / tw, j1 - j0);
-    else lc = c;
-    spiece[i] = make_uint3(v, j0, j1);
-    sblk[i] = pblk[q];
-    kC[i] = kc;
-    kW[i] = kw;
-    lcost[i] = lc;  // 0: not a light piece (a light piece costs at least 1)
+    const uint64_t nin = inptr[v + 1] - inptr[v];
+    uint8_t cls = kClassNone;
+    uint64_t cl = 0;
+    uint32_t kw = 0, kc = 0;
+    if (dv && nin) {
+      // a warp holds N+(v) as a bitmap when its id span is short, else as
+      // buckets when d+(v) <= warp_cap; otherwise the CTA shares one set
+      const uint32_t span = adj[(uint64_t)rv.x * 4 + dv - 1] - adj[(uint64_t)rv.x * 4];
+      const bool bitmap = span <= bitmap_max_span(kWarpTableSlots);
+      const bool warp_fits = bitmap || dv <= pp.warp_cap;
+      const uint64_t build = bitmap ? (span >> 5) + dv : 4ull * dv;
+      const bool pred = pcost && warp_fits;
+      const uint64_t c = pred ? pcost[v] + 1 : work[v] + build + pp.vertex_overhead;
+      const uint64_t tw = pred ? tw_pred : pp.warp_tile_cost;
+      if (!warp_fits) {
+        cls = kClassCta;
+        kc = (uint32_t)min_u64((c + pp.cta_tile_cost - 1) / pp.cta_tile_cost, nin);
+      } else if (c > tw) {
+        cls = kClassSplit;
+        kw = (uint32_t)min_u64((c + tw - 1) / tw, nin);
+      } else {
+        cls = kClassLight;
+        cl = c;
+      }
+    }
+    vclass[v] = cls;
+    costL[v] = cl;
+    kW[v] = kw;
+    kC[v] = kc;
   }
 }
 
-// The off[i+1] - off[i] tiles of piece i (off: exclusive scan of the tile
-// counts), its record range cut evenly, at tiles[off[i] + shift[block] ..]
-// (no shift for CTA tiles, which are laid out in block order already).
-__global__ void k_fill_piece_tiles(const uint3 *__restrict__ spiece, const uint32_t *__restrict__ sblk,
-                                   uint32_t np, const uint32_t *__restrict__ off,
-                                   const int64_t *__restrict__ shift, Tile *__restrict__ tiles) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < np;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t kk = off[i + 1] - off[i];
+// off[] holds exclusive tile offsets (n+1 entries): vertex v owns tiles
+// off[v] .. off[v+1], splitting its in-edge list evenly.
+__global__ void k_fill_split_tiles(const uint64_t *__restrict__ inptr, uint32_t n,
+                                   const uint32_t *__restrict__ off, Tile *__restrict__ tiles) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t kk = off[v + 1] - off[v];
     if (!kk) continue;
-    const uint3 pc = spiece[i];
-    const uint32_t nrec = pc.z - pc.y;
-    const int64_t o = (int64_t)off[i] + (shift ? shift[sblk[i]] : 0);
-    for (uint32_t t = 0; t < kk; ++t) {
-      Tile tl;
-      tl.v0 = pc.x;
-      tl.v1 = pc.x + 1;
-      tl.j0 = pc.y + (uint32_t)((uint64_t)t * nrec / kk);
-      tl.j1 = pc.y + (uint32_t)((uint64_t)(t + 1) * nrec / kk);
-      tiles[o + t] = tl;
+    const uint64_t nin = inptr[v + 1] - inptr[v];
+    const uint32_t o = off[v];
+    for (uint32_t i = 0; i < kk; ++i) {
+      Tile t;
+      t.v0 = (uint32_t)v;
+      t.v1 = (uint32_t)v + 1;
+      t.j0 = (uint32_t)((uint64_t)i * nin / kk);
+      t.j1 = (uint32_t)((uint64_t)(i + 1) * nin / kk);
+      tiles[o + i] = t;
     }
   }
 }
@@ -261,31 +182,19 @@ struct GroupTarget {
   __host__ __device__ uint64_t operator()(uint64_t g) const { return g * tw; }
 };
 
-struct IsLightPiece {
-  const uint64_t *lcost;
-  __host__ __device__ bool operator()(uint32_t i) const { return lcost[i] != 0; }
+struct IsLight {
+  const uint8_t *vclass;
+  __host__ __device__ bool operator()(uint32_t v) const { return vclass[v] == kClassLight; }
 };
 
-struct PieceAt {
-  const uint3 *spiece;
-  __host__ __device__ uint3 operator()(uint32_t i) const { return spiece[i]; }
+struct LightCost {
+  const uint64_t *cost;
+  __host__ __device__ uint64_t operator()(uint32_t v) const { return cost[v]; }
 };
 
-struct BlockAt {
-  const uint32_t *sblk;
-  __host__ __device__ uint32_t operator()(uint32_t i) const { return sblk[i]; }
-};
-
-struct CostAt {
-  const uint64_t *lcost;
-  __host__ __device__ uint64_t operator()(uint32_t i) const { return lcost[i]; }
-};
-
-// Group tiles over the light-piece list: group g covers positions
-// [starts[g], starts[g+1]); it belongs to the block of its first piece and
-// lands after that block's split tiles.
+// Group tiles over the compacted light-vertex list: tile g covers list
+// positions [starts[g], starts[g+1]).
 __global__ void k_fill_group_tiles(const uint32_t *__restrict__ starts, uint64_t G, uint32_t L,
-                                   const uint32_t *__restrict__ lblk, const int64_t *__restrict__ gbase,
                                    Tile *__restrict__ tiles) {
   for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G;
        g += (uint64_t)gridDim.x * blockDim.x) {
@@ -294,7 +203,7 @@ __global__ void k_fill_group_tiles(const uint32_t *__restrict__ starts, uint64_t
     t.v1 = g + 1 < G ? starts[g + 1] : L;
     t.j0 = 0;
     t.j1 = kGroupTile;
-    tiles[gbase[lblk[t.v0]] + (int64_t)g] = t;
+    tiles[g] = t;
   }
 }
 
@@ -371,11 +280,7 @@ __global__ void k_predict(const float *__restrict__ params, const float *__restr
 
 namespace {
 
-// The in-edge index with every vertex's records grouped by source block
-// (blocks of `bw` words of adj), and per record its {vertex, block} in recvp
-// (scratch for the piece pass).  ublk receives the P + 1 block row bounds.
-int build_in_index(gary_graph *g, cudaStream_t s, uint64_t bw, InIndex &in, DevBuf<uint2> &recvp,
-                   std::vector<uint32_t> &ublk) {
+int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
   const uint32_t n = g->n;
   const uint64_t W = g->dag.words;
   if (W >= (1ull << 32)) {
@@ -384,28 +289,15 @@ int build_in_index(gary_graph *g, cudaStream_t s, uint64_t bw, InIndex &in, DevB
   }
   ScratchAlloc pol_alloc{s};
   auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
-  const uint32_t P = (uint32_t)std::max<uint64_t>((W + bw - 1) / bw, 1);
-  {
-    DevBuf<uint32_t> dub;
-    GARY_TRY(dub.alloc((uint64_t)P + 1, s));
-    k_block_rows<<<grid_for((uint64_t)P + 1), kThreads, 0, s>>>(g->dag.row.p, n, bw, P, dub.p);
-    GARY_CUDA(cudaGetLastError());
-    ublk.resize((size_t)P + 1);
-    GARY_CUDA(cudaMemcpyAsync(ublk.data(), dub.p, ((size_t)P + 1) * 4, cudaMemcpyDeviceToHost, s));
-    GARY_CUDA(cudaStreamSynchronize(s));
-  }
   DevBuf<uint32_t> cnt, slot;
   GARY_TRY(cnt.alloc((uint64_t)n + 1, s));
   GARY_TRY(slot.alloc(std::max<uint64_t>(W, 1), s));
   GARY_TRY(in.work.alloc_persistent(n));
   GARY_CUDA(cudaMemsetAsync(cnt.p, 0, ((uint64_t)n + 1) * 4, s));
   GARY_CUDA(cudaMemsetAsync(in.work.p, 0, (uint64_t)n * 8, s));
-  for (uint32_t p = 0; p < P; ++p) {  // block by block: slots in block order
-    if (ublk[p + 1] <= ublk[p]) continue;
-    k_in_count<<<grid_for(ublk[p + 1] - ublk[p]), kThreads, 0, s>>>(
-        g->dag.row.p, g->dag.adj.p, ublk[p], ublk[p + 1], cnt.p,
-        reinterpret_cast<unsigned long long *>(in.work.p), slot.p);
-  }
+  const unsigned grid = grid_for((uint64_t)n);  // one warp per 32 rows
+  k_in_count<<<grid, kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, n, cnt.p,
+                                       reinterpret_cast<unsigned long long *>(in.work.p), slot.p);
   GARY_CUDA(cudaGetLastError());
   GARY_TRY(in.inptr.alloc_persistent((uint64_t)n + 1));
   auto wide = thrust::make_transform_iterator(cnt.p, U32ToU64());
@@ -416,13 +308,10 @@ int build_in_index(gary_graph *g, cudaStream_t s, uint64_t bw, InIndex &in, DevB
   cnt.release();
   in.records = m;
   GARY_TRY(in.inedge.alloc_persistent(std::max<uint64_t>(m, 1)));
-  GARY_TRY(recvp.alloc(std::max<uint64_t>(m, 1), s));
-  for (uint32_t p = 0; p < P && m; ++p) {
-    if (ublk[p + 1] <= ublk[p]) continue;
-    k_in_fill<<<grid_for(ublk[p + 1] - ublk[p]), kThreads, 0, s>>>(
-        g->dag.row.p, g->dag.adj.p, ublk[p], ublk[p + 1], p, in.inptr.p, slot.p, in.inedge.p, recvp.p);
+  if (m) {
+    k_in_fill<<<grid, kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, n, in.inptr.p, slot.p, in.inedge.p);
+    GARY_CUDA(cudaGetLastError());
   }
-  GARY_CUDA(cudaGetLastError());
   in.total_work = thrust::reduce(pol, in.work.p, in.work.p + n, 0ull);
   return GARY_OK;
 }
@@ -453,65 +342,16 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp_in, cudaStream_t s, gary_c
   ScratchAlloc pol_alloc{s};
   auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
   PhaseTrace tr("triangle plan", s);
-  // source blocks of kSrcBlockWords words (the lists one block reads stay in
-  // L2); a graph whose lists fit twice that is one block
-  const uint64_t W = g->dag.words;
-  uint64_t bw = pp_in.src_block_words ? pp_in.src_block_words : kSrcBlockWords;
-  if (!pp_in.src_block_words && W <= 2 * kSrcBlockWords) bw = std::max<uint64_t>(W, 1);
-  DevBuf<uint2> recvp;
-  std::vector<uint32_t> ublk;
-  GARY_TRY(build_in_index(g, s, bw, plan->in, recvp, ublk));
-  const uint32_t P = (uint32_t)ublk.size() - 1;
-  plan->nblocks = P;
+  GARY_TRY(build_in_index(g, s, plan->in));
   tr.mark("in-edge index");
-  PlanParams pp = resolve_params(pp_in, plan->in.total_work);
-  pp.src_block_words = bw;
+  const PlanParams pp = resolve_params(pp_in, plan->in.total_work);
   plan->params = pp;
-  const uint64_t m = plan->in.records;
-
-  // pieces: the records of one vertex from one block (contiguous, in vertex order)
-  DevBuf<uint32_t> pid, pv, pblk, pj0;
-  DevBuf<unsigned long long> pwork;
-  uint32_t np = 0;
-  {
-    GARY_TRY(pid.alloc(m + 1, s));
-    k_piece_heads<<<grid_for(m + 1), kThreads, 0, s>>>(recvp.p, m, pid.p);
-    GARY_CUDA(cudaGetLastError());
-    thrust::exclusive_scan(pol, pid.p, pid.p + m + 1, pid.p, 0u);
-    GARY_CUDA(cudaMemcpyAsync(&np, pid.p + m, 4, cudaMemcpyDeviceToHost, s));
-    GARY_CUDA(cudaStreamSynchronize(s));
-    GARY_TRY(pv.alloc(std::max<uint32_t>(np, 1), s));
-    GARY_TRY(pblk.alloc(std::max<uint32_t>(np, 1), s));
-    GARY_TRY(pj0.alloc(std::max<uint32_t>(np, 1), s));
-    GARY_TRY(pwork.alloc(std::max<uint32_t>(np, 1), s));
-    GARY_CUDA(cudaMemsetAsync(pwork.p, 0, (uint64_t)std::max<uint32_t>(np, 1) * 8, s));
-    if (m)
-      k_piece_fill<<<grid_for(m), kThreads, 0, s>>>(recvp.p, plan->in.inedge.p, plan->in.inptr.p, m, pid.p,
-                                                    pv.p, pblk.p, pj0.p, pwork.p);
-    GARY_CUDA(cudaGetLastError());
-    pid.release();
-    recvp.release();
-  }
-  // block order (stable: vertices ascending within a block)
-  DevBuf<uint32_t> order;
-  GARY_TRY(order.alloc(std::max<uint32_t>(np, 1), s));
-  if (np) {
-    DevBuf<uint32_t> kin, kout, vin;
-    GARY_TRY(kin.alloc(np, s));
-    GARY_TRY(kout.alloc(np, s));
-    GARY_TRY(vin.alloc(np, s));
-    GARY_CUDA(cudaMemcpyAsync(kin.p, pblk.p, (uint64_t)np * 4, cudaMemcpyDeviceToDevice, s));
-    thrust::sequence(pol, vin.p, vin.p + np, 0u);
-    int eb = 1;
-    while (eb < 32 && ((uint64_t)P - 1) >> eb) ++eb;
-    size_t tmp = 0;
-    GARY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kin.p, kout.p, vin.p, order.p, (int)np, 0, eb, s));
-    DevBuf<uint8_t> t;
-    GARY_TRY(t.alloc(std::max<size_t>(tmp, 1), s));
-    GARY_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kin.p, kout.p, vin.p, order.p, (int)np, 0, eb, s));
-  }
-  tr.mark("pieces");
-
+  GARY_TRY(plan->vclass.alloc_persistent(n));
+  DevBuf<uint64_t> costV;  // cost of each light vertex, 0 for the others
+  DevBuf<uint32_t> kW, kC;
+  GARY_TRY(costV.alloc(n, s));
+  GARY_TRY(kW.alloc((uint64_t)n + 1, s));
+  GARY_TRY(kC.alloc((uint64_t)n + 1, s));
   // learned plans: per-vertex features -> cost model -> variant and predicted cycles
   DevBuf<uint64_t> pcost;
   uint64_t tw = pp.warp_tile_cost;
@@ -534,128 +374,53 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp_in, cudaStream_t s, gary_c
     tw = std::max<uint64_t>(total / std::max<uint64_t>(slots, 1), 4096);
     plan->learned = true;
   }
-
-  // classify the pieces (block order), tile counts and light costs
-  DevBuf<uint3> spiece;
-  DevBuf<uint32_t> sblk, kC, kW;
-  DevBuf<uint64_t> lcost;
-  GARY_TRY(spiece.alloc(std::max<uint32_t>(np, 1), s));
-  GARY_TRY(sblk.alloc(std::max<uint32_t>(np, 1), s));
-  GARY_TRY(kC.alloc((uint64_t)np + 1, s));
-  GARY_TRY(kW.alloc((uint64_t)np + 1, s));
-  GARY_TRY(lcost.alloc(std::max<uint32_t>(np, 1), s));
-  if (np)
-    k_classify_pieces<<<grid_for(np), kThreads, 0, s>>>(
-        g->dag.row.p, g->dag.adj.p, plan->in.inptr.p, plan->in.work.p, order.p, np, pv.p, pblk.p, pj0.p,
-        pwork.p, pp, model ? pcost.p : nullptr, tw, spiece.p, sblk.p, kC.p, kW.p, lcost.p);
+  k_classify<<<grid_for(n), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, plan->in.work.p, plan->in.inptr.p, n, pp,
+                                              model ? pcost.p : nullptr, tw, plan->vclass.p, costV.p, kW.p,
+                                              kC.p);
   GARY_CUDA(cudaGetLastError());
-  GARY_CUDA(cudaMemsetAsync(kC.p + np, 0, 4, s));
-  GARY_CUDA(cudaMemsetAsync(kW.p + np, 0, 4, s));
-  thrust::exclusive_scan(pol, kC.p, kC.p + np + 1, kC.p, 0u);
-  thrust::exclusive_scan(pol, kW.p, kW.p + np + 1, kW.p, 0u);
-  order.release();
-  pv.release();
-  pblk.release();
-  pj0.release();
-  pwork.release();
-
-  // light pieces (block order) and their group tiles
-  uint32_t L = 0;
-  uint64_t G = 0;
-  DevBuf<uint32_t> lidx, lblk, starts, gblk;
-  if (np) {
-    GARY_TRY(lidx.alloc(np, s));
-    L = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
-                                   thrust::counting_iterator<uint32_t>(np), lidx.p, IsLightPiece{lcost.p}) -
-                   lidx.p);
-  }
-  plan->n_light = L;
-  if (L) {
-    GARY_TRY(plan->lpieces.alloc_persistent(L));
-    GARY_TRY(lblk.alloc(L, s));
-    thrust::transform(pol, lidx.p, lidx.p + L, plan->lpieces.p, PieceAt{spiece.p});
-    thrust::transform(pol, lidx.p, lidx.p + L, lblk.p, BlockAt{sblk.p});
-    // lc[i] = cost of the light pieces before position i (lc[L] = their total)
-    DevBuf<uint64_t> lc;
-    GARY_TRY(lc.alloc((uint64_t)L + 1, s));
-    GARY_CUDA(cudaMemsetAsync(lc.p, 0, 8, s));
-    auto costs = thrust::make_transform_iterator(lidx.p, CostAt{lcost.p});
-    thrust::inclusive_scan(pol, costs, costs + L, lc.p + 1);
-    uint64_t totalL = 0;
-    GARY_CUDA(cudaMemcpyAsync(&totalL, lc.p + L, 8, cudaMemcpyDeviceToHost, s));
-    GARY_CUDA(cudaStreamSynchronize(s));
-    G = (totalL + tw - 1) / tw;
-    GARY_TRY(starts.alloc(G, s));
-    auto targets = thrust::make_transform_iterator(thrust::counting_iterator<uint64_t>(0), GroupTarget{tw});
-    thrust::lower_bound(pol, lc.p, lc.p + L, targets, targets + G, starts.p);
-    GARY_TRY(gblk.alloc(G, s));
-    thrust::transform(pol, starts.p, starts.p + G, gblk.p, BlockAt{lblk.p});
-  }
-  lidx.release();
-
-  // per-block tile ranges: CTA tiles [cta_off[p], cta_off[p+1]), warp tiles
-  // [warp_off[p], warp_off[p+1]) = the block's split tiles, then its groups
-  uint32_t nC = 0, nWs = 0;
-  GARY_CUDA(cudaMemcpyAsync(&nC, kC.p + np, 4, cudaMemcpyDeviceToHost, s));
-  GARY_CUDA(cudaMemcpyAsync(&nWs, kW.p + np, 4, cudaMemcpyDeviceToHost, s));
-  std::vector<uint32_t> pfirst(P + 1), gfirst(P + 1, 0);
-  {
-    DevBuf<uint32_t> keys, res;
-    GARY_TRY(keys.alloc((uint64_t)P + 1, s));
-    GARY_TRY(res.alloc((uint64_t)P + 1, s));
-    thrust::sequence(pol, keys.p, keys.p + P + 1, 0u);
-    thrust::lower_bound(pol, sblk.p, sblk.p + np, keys.p, keys.p + P + 1, res.p);
-    GARY_CUDA(cudaMemcpyAsync(pfirst.data(), res.p, ((size_t)P + 1) * 4, cudaMemcpyDeviceToHost, s));
-    GARY_CUDA(cudaStreamSynchronize(s));
-    if (G) {
-      thrust::lower_bound(pol, gblk.p, gblk.p + G, keys.p, keys.p + P + 1, res.p);
-      GARY_CUDA(cudaMemcpyAsync(gfirst.data(), res.p, ((size_t)P + 1) * 4, cudaMemcpyDeviceToHost, s));
-    }
-  }
-  std::vector<uint32_t> kCat(P + 1), kWat(P + 1);
-  for (uint32_t p = 0; p <= P; ++p) {
-    GARY_CUDA(cudaMemcpyAsync(&kCat[p], kC.p + pfirst[p], 4, cudaMemcpyDeviceToHost, s));
-    GARY_CUDA(cudaMemcpyAsync(&kWat[p], kW.p + pfirst[p], 4, cudaMemcpyDeviceToHost, s));
-  }
+  GARY_CUDA(cudaMemsetAsync(kW.p + n, 0, 4, s));
+  GARY_CUDA(cudaMemsetAsync(kC.p + n, 0, 4, s));
+  const uint64_t totalL = thrust::reduce(pol, costV.p, costV.p + n, 0ull);
+  thrust::exclusive_scan(pol, kW.p, kW.p + n + 1, kW.p, 0u);
+  thrust::exclusive_scan(pol, kC.p, kC.p + n + 1, kC.p, 0u);
+  uint32_t nW = 0, nC = 0;
+  GARY_CUDA(cudaMemcpyAsync(&nW, kW.p + n, 4, cudaMemcpyDeviceToHost, s));
+  GARY_CUDA(cudaMemcpyAsync(&nC, kC.p + n, 4, cudaMemcpyDeviceToHost, s));
   GARY_CUDA(cudaStreamSynchronize(s));
-  const uint64_t total = (uint64_t)nC + nWs + G;
+  tr.mark("classify");
+  const uint64_t G = totalL ? (totalL + tw - 1) / tw : 0;
+  const uint64_t total = (uint64_t)nC + nW + G;
   if (total >= (1ull << 31)) {
     set_error("tile plan too large (%llu tiles)", (unsigned long long)total);
     return GARY_ERR_UNSUPPORTED;
   }
-  std::vector<uint32_t> blkoff(2 * ((size_t)P + 1));
-  std::vector<int64_t> split_shift(P), group_base(P);
-  uint32_t wo = 0;
-  for (uint32_t p = 0; p < P; ++p) {
-    blkoff[p] = kCat[p];
-    blkoff[P + 1 + p] = wo;
-    const uint32_t splits = kWat[p + 1] - kWat[p];
-    const uint32_t groups = gfirst[p + 1] - gfirst[p];
-    split_shift[p] = (int64_t)nC + wo - kWat[p];
-    group_base[p] = (int64_t)nC + wo + splits - gfirst[p];
-    wo += splits + groups;
-  }
-  blkoff[P] = nC;
-  blkoff[2 * P + 1] = wo;
   plan->n_cta = nC;
-  plan->n_warp = wo;
-  plan->blkoff_h = blkoff;
-  GARY_TRY(plan->blkoff.alloc_persistent(blkoff.size()));
-  GARY_CUDA(cudaMemcpyAsync(plan->blkoff.p, blkoff.data(), blkoff.size() * 4, cudaMemcpyHostToDevice, s));
-  GARY_TRY(plan->queue.alloc_persistent(2 * (uint64_t)P));
+  plan->n_warp = (uint32_t)(nW + G);
   GARY_TRY(plan->tiles.alloc_persistent(std::max<uint64_t>(total, 1)));
-  DevBuf<int64_t> dshift, dgbase;
-  GARY_TRY(dshift.alloc(P, s));
-  GARY_TRY(dgbase.alloc(P, s));
-  GARY_CUDA(cudaMemcpyAsync(dshift.p, split_shift.data(), (size_t)P * 8, cudaMemcpyHostToDevice, s));
-  GARY_CUDA(cudaMemcpyAsync(dgbase.p, group_base.data(), (size_t)P * 8, cudaMemcpyHostToDevice, s));
-  if (np) {
-    k_fill_piece_tiles<<<grid_for(np), kThreads, 0, s>>>(spiece.p, sblk.p, np, kC.p, nullptr, plan->tiles.p);
-    k_fill_piece_tiles<<<grid_for(np), kThreads, 0, s>>>(spiece.p, sblk.p, np, kW.p, dshift.p, plan->tiles.p);
-  }
-  if (G)
-    k_fill_group_tiles<<<grid_for(G), kThreads, 0, s>>>(starts.p, G, L, lblk.p, dgbase.p, plan->tiles.p);
+  k_fill_split_tiles<<<grid_for(n), kThreads, 0, s>>>(plan->in.inptr.p, n, kC.p, plan->tiles.p);
+  k_fill_split_tiles<<<grid_for(n), kThreads, 0, s>>>(plan->in.inptr.p, n, kW.p,
+                                                     plan->tiles.p + nC);
   GARY_CUDA(cudaGetLastError());
+  if (G) {
+    // light vertices in id order, and the exclusive prefix of their costs
+    GARY_TRY(plan->light.alloc_persistent(n));
+    const uint32_t L = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
+                                                  thrust::counting_iterator<uint32_t>(n),
+                                                  plan->light.p, IsLight{plan->vclass.p}) -
+                                  plan->light.p);
+    plan->n_light = L;
+    DevBuf<uint64_t> lc;
+    GARY_TRY(lc.alloc((uint64_t)L + 1, s));
+    auto costs = thrust::make_transform_iterator(plan->light.p, LightCost{costV.p});
+    thrust::exclusive_scan(pol, costs, costs + L, lc.p, 0ull);
+    DevBuf<uint32_t> starts;
+    GARY_TRY(starts.alloc(G, s));
+    auto targets = thrust::make_transform_iterator(thrust::counting_iterator<uint64_t>(0),
+                                                   GroupTarget{tw});
+    thrust::lower_bound(pol, lc.p, lc.p + L, targets, targets + G, starts.p);
+    k_fill_group_tiles<<<grid_for(G), kThreads, 0, s>>>(starts.p, G, L, plan->tiles.p + nC + nW);
+    GARY_CUDA(cudaGetLastError());
+  }
   GARY_TRY(plan->sched.alloc_persistent(1));
   GARY_CUDA(cudaStreamSynchronize(s));
   tr.mark("tiles");
@@ -938,9 +703,8 @@ __device__ __forceinline__ uint32_t warp_vertex(const GraphView &g, const uint2 
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     k_tc_mid(GraphView g, const uint2 *__restrict__ inedge, const uint64_t *__restrict__ inptr,
-             const uint3 *__restrict__ lpieces, const Tile *__restrict__ tiles, uint32_t n_cta,
-             const uint32_t *__restrict__ blkoff, uint32_t nblocks, uint32_t shard, uint32_t nshards,
-             uint32_t *queue, SchedState *sched, unsigned long long *__restrict__ out, VertexCtl ctl,
+             const uint32_t *__restrict__ light, const Tile *__restrict__ tiles, uint32_t n_cta,
+             TileRange rng, SchedState *sched, unsigned long long *__restrict__ out, VertexCtl ctl,
              CtaSetCfg cfg) {
   extern __shared__ __align__(16) uint32_t smem[];
   __shared__ uint64_t bar;
@@ -955,63 +719,44 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   }
   __syncthreads();
   uint32_t phase = 0;
+
+  // phase 1: CTA tiles (N+(v) does not fit a warp's set)
+  bool alive = true;
+  while (true) {
+    if (threadIdx.x == 0) s_tile = rng.cta_lo + atomicAdd(&sched->next_cta, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    __syncthreads();
+    if (t >= rng.cta_hi) break;
+    const Tile tl = tiles[t];
+    if (!cta_tile<WARPS>(g, inedge, inptr, tl, smem, &s_chunk, &bar, phase, cfg, sched, ctl.gid,
+                         ctl.gcount, cnt)) {
+      alive = false;  // a staging copy may still land in shared memory: no more work here
+      break;
+    }
+  }
+
+  // phase 2: warp tiles, each warp on its own slots
   uint32_t *tab = smem + warp * kWarpTableSlots;
   const Tile *wt = tiles + n_cta;
-  auto part = [&](uint32_t a, uint32_t b, uint32_t k) {  // shard k's share of [a, b)
-    return a + (uint32_t)((uint64_t)(b - a) * k / nshards);
-  };
-
-  // source blocks one after another: the lists a block's tiles read stay in L2
-  bool alive = true;
-  for (uint32_t p = 0; p < nblocks && alive; ++p) {
-    // CTA tiles (N+(v) does not fit a warp's set)
-    while (true) {
-      if (threadIdx.x == 0) {
-        const uint32_t c0 = blkoff[p], c1 = blkoff[p + 1];
-        const uint32_t t = part(c0, c1, shard) + atomicAdd(&queue[2 * p], 1u);
-        s_tile = t < part(c0, c1, shard + 1) ? t : 0xFFFFFFFFu;
-      }
-      __syncthreads();
-      const uint32_t t = s_tile;
-      __syncthreads();
-      if (t == 0xFFFFFFFFu) break;
-      const Tile tl = tiles[t];
-      if (!cta_tile<WARPS>(g, inedge, inptr, tl, smem, &s_chunk, &bar, phase, cfg, sched, ctl.gid,
-                           ctl.gcount, cnt)) {
-        alive = false;  // a staging copy may still land in shared memory: no more work here
-        break;
-      }
+  while (alive) {
+    uint32_t t = 0;
+    if (lane == 0) t = rng.warp_lo + atomicAdd(&sched->next_warp, 1u);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= rng.warp_hi) break;
+    const Tile tl = wt[t];
+    if (tl.j1 != kGroupTile) {
+      cnt += warp_vertex(g, inedge, inptr, tl.v0, tl.j0, tl.j1, tab, lane, ctl);
+      continue;
     }
-    if (!alive) break;
-
-    // warp tiles, each warp on its own slots
-    while (true) {
-      uint32_t t = 0;
-      if (lane == 0) {
-        const uint32_t w0 = blkoff[nblocks + 1 + p], w1 = blkoff[nblocks + 2 + p];
-        t = part(w0, w1, shard) + atomicAdd(&queue[2 * p + 1], 1u);
-        if (t >= part(w0, w1, shard + 1)) t = 0xFFFFFFFFu;
-      }
-      t = __shfl_sync(kFull, t, 0);
-      if (t == 0xFFFFFFFFu) break;
-      const Tile tl = wt[t];
-      if (tl.j1 != kGroupTile) {
-        cnt += warp_vertex(g, inedge, inptr, tl.v0, tl.j0, tl.j1, tab, lane, ctl);
-        continue;
-      }
-      // a group of light pieces: list positions [v0, v1), 32 pieces per load
-      for (uint32_t ib = tl.v0; ib < tl.v1; ib += 32) {
-        const uint32_t nb = min(32u, tl.v1 - ib);
-        const uint3 mp = lane < nb ? lpieces[ib + lane] : make_uint3(0, 0, 0);
-        for (uint32_t k = 0; k < nb; ++k)
-          cnt += warp_vertex(g, inedge, inptr, __shfl_sync(kFull, mp.x, k), __shfl_sync(kFull, mp.y, k),
-                             __shfl_sync(kFull, mp.z, k), tab, lane, ctl);
-      }
+    // a group of light vertices: list positions [v0, v1), 32 ids per load
+    for (uint32_t ib = tl.v0; ib < tl.v1; ib += 32) {
+      const uint32_t nb = min(32u, tl.v1 - ib);
+      const uint32_t myv = lane < nb ? light[ib + lane] : 0u;
+      for (uint32_t k = 0; k < nb; ++k)
+        cnt += warp_vertex(g, inedge, inptr, __shfl_sync(kFull, myv, k), 0, 0xFFFFFFFFu, tab, lane,
+                           ctl);
     }
-    // every warp is done with its slots before the next block's CTA tiles,
-    // which may fill shared memory through the async proxy
-    fence_proxy_async_smem();
-    __syncthreads();
   }
 
   cnt = warp_sum_u64(cnt);
@@ -1048,6 +793,7 @@ int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_o
   const unsigned grid = (unsigned)std::min<int>(sm_count() * per_sm, (int)kMaxCountCtas);
   if (!plan->span.p) GARY_TRY(plan->span.alloc_persistent(2 * kMaxCountCtas));
   ctl.span = plan->span.p;
+  const TileRange rng = shard_range(plan->n_cta, plan->n_warp, shard, nshards);
   const uint32_t words = (uint32_t)(WARPS * kWarpTableSlots);
   const uint32_t cw = plan->params.cta_set_words;
   const CtaSetCfg cfg{cw && cw < words ? cw : words, plan->params.stage_polls};
@@ -1056,26 +802,15 @@ int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_o
   const bool timed = cap == cudaStreamCaptureStatusNone;
   GARY_CUDA(cudaMemsetAsync(plan->sched.p, 0, sizeof(SchedState), s));
   GARY_CUDA(cudaMemsetAsync(plan->span.p, 0, 2ull * grid * 8, s));
-  GARY_CUDA(cudaMemsetAsync(plan->queue.p, 0, 2ull * plan->nblocks * 4, s));
   GARY_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), s));
   if (timed) GARY_CUDA(cudaEventRecord(g->ev0, s));
-  kern<<<grid, WARPS * 32, smem, s>>>(g->view(), plan->in.inedge.p, plan->in.inptr.p, plan->lpieces.p,
-                                      plan->tiles.p, plan->n_cta, plan->blkoff.p, plan->nblocks, shard,
-                                      nshards, plan->queue.p, plan->sched.p, d_out, ctl, cfg);
+  kern<<<grid, WARPS * 32, smem, s>>>(g->view(), plan->in.inedge.p, plan->in.inptr.p, plan->light.p,
+                                      plan->tiles.p, plan->n_cta, rng, plan->sched.p, d_out, ctl, cfg);
   GARY_CUDA(cudaGetLastError());
   if (timed) GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
-  // this shard's tiles: its share of every block's ranges
-  uint32_t nct = 0, nwt = 0;
-  const uint32_t P = plan->nblocks;
-  const std::vector<uint32_t> &bo = plan->blkoff_h;
-  for (uint32_t p = 0; p < P; ++p) {
-    const uint64_t c = bo[p + 1] - bo[p], w = bo[P + 2 + p] - bo[P + 1 + p];
-    nct += (uint32_t)(c * (shard + 1) / nshards - c * shard / nshards);
-    nwt += (uint32_t)(w * (shard + 1) / nshards - w * shard / nshards);
-  }
-  g->last.tiles = nct + nwt;
-  g->last.cta_tiles = nct;
+  g->last.tiles = (rng.cta_hi - rng.cta_lo) + (rng.warp_hi - rng.warp_lo);
+  g->last.cta_tiles = rng.cta_hi - rng.cta_lo;
   g->last.work = plan->in.total_work;
   g->last_timed = timed;
   g->last_sched = plan->sched.p;

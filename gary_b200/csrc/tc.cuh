@@ -1,7 +1,6 @@
 // Tile plans and launch entry points of the counting kernels.
 #pragma once
 #include <cstdint>
-#include <vector>
 
 #include "bulk.cuh"
 #include "graph.cuh"
@@ -13,9 +12,6 @@ constexpr int kTcWarps = 16;               // warps per CTA of the counting kern
 constexpr uint32_t kWarpTableSlots = 1024;  // per-warp shared set (4 KB)
 constexpr uint32_t kGroupTile = 0xFFFFFFFFu;
 constexpr uint32_t kMaxCountCtas = 1024;  // CTAs of a counting launch (SMs x resident CTAs)
-// Words of adjacency per source block of the triangle plan (48 MB: the lists
-// one block reads stay in the 126 MB L2 beside the other streams).
-constexpr uint64_t kSrcBlockWords = 12ull << 20;
 
 enum : uint8_t { kClassNone = 0, kClassLight = 1, kClassSplit = 2, kClassCta = 3 };
 
@@ -35,8 +31,8 @@ __host__ __device__ __forceinline__ bool variant_legal(uint32_t var, uint32_t d,
 }
 
 // A unit of scheduled work over middle vertices v.
-//   j1 == kGroupTile : light pieces lpieces[v0 .. v1) (the plan's list of
-//                      light pieces {v, j0, j1})
+//   j1 == kGroupTile : light vertices light[v0 .. v1) (the plan's compacted
+//                      list of light vertices), all their in-edges
 //   otherwise        : vertex v0 only, in-edges [j0, j1) of its in-list
 struct Tile {
   uint32_t v0, v1, j0, j1;
@@ -60,8 +56,6 @@ struct PlanParams {
   uint32_t min_blocks = 0;                  // resident CTAs per SM, 2 or 3 (0: from the work)
   uint32_t cta_set_words = 0;               // 0: the CTA's whole shared buffer
   uint32_t stage_polls = kSpinLimit;        // polls of the first staging wait
-  uint64_t src_block_words = 0;             // words per source block (0: kSrcBlockWords, and
-                                            // one block when the lists fit in two)
 };
 
 // The parameters a plan over `total_work` probes uses: explicit values as
@@ -112,23 +106,11 @@ struct InIndex {
 
 }  // namespace gary
 
-// The triangle plan.  The adjacency is cut into source blocks (rows of
-// consecutive vertices, ~kSrcBlockWords words each); the records of a middle
-// vertex v from one block form a piece.  Tiles cover pieces and are laid out
-// block by block: CTA tiles (vertices whose N+(v) fits no warp set) in
-// tiles[0, n_cta), warp tiles (split pieces, then group tiles of light
-// pieces) in tiles[n_cta, n_cta + n_warp).  Block p's CTA tiles are
-// [blkoff[p], blkoff[p+1]) and its warp tiles [blkoff[P+1+p], blkoff[P+2+p])
-// of the warp part.  The kernel runs the blocks in order, so the lists one
-// block's tiles read stay in L2.
 struct gary_count_plan {
   gary::PlanParams params;
   gary::InIndex in;
-  uint32_t nblocks = 1;
-  gary::DevBuf<uint32_t> blkoff;   // 2 (P + 1) tile offsets (see above)
-  std::vector<uint32_t> blkoff_h;  // host copy
-  gary::DevBuf<uint32_t> queue;    // 2 P tile counters, zeroed per launch
-  gary::DevBuf<uint3> lpieces;     // light pieces {v, j0, j1} (group tiles index this list)
+  gary::DevBuf<uint8_t> vclass;
+  gary::DevBuf<uint32_t> light;  // light vertices (group tiles index this list)
   uint32_t n_light = 0;
   gary::DevBuf<gary::Tile> tiles;
   uint32_t n_cta = 0;

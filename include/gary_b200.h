@@ -238,11 +238,6 @@ int gary_gen_ba(uint32_t n, uint32_t m, uint64_t seed, uint32_t *src, uint32_t *
  *   "vertex_overhead" fixed cost charged per vertex      (default 64)
  *   "min_blocks"      resident CTAs per SM, 2 or 3; 0 (the default) picks 3
  *                     from 2^31 probes on, else 2
- *   "src_block_bytes" bytes of adjacency per source block of the triangle plan
- *                     (the kernel runs the blocks one after another so that the
- *                     lists one block reads stay in L2); 0 (the default) takes
- *                     48 MB, and one block when the lists fit in 96 MB; else at
- *                     least 2^20 and a multiple of 32
  *   "warp_cap"        largest out-degree d+(v) a warp's hash set takes
  *                     (8..512, default 512); larger lists whose id span is
  *                     too wide for a warp bitmap go to CTA tiles

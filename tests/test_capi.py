@@ -92,12 +92,10 @@ def test_tuning_keys_checked():
     try:
         for key, bad in (("warp_cap", 4), ("warp_cap", 1024), ("cta_set_words", 100), ("cta_set_words", 32),
                          ("cta_set_words", 32768), ("stage_wait_polls", (1 << 24) + 1), ("min_blocks", 1),
-                         ("src_block_bytes", 4096), ("src_block_bytes", (1 << 20) + 4),
                          ("no_such_key", 1)):
             assert L.gary_tune(key.encode(), bad) == _lib.GARY_ERR_INVALID, (key, bad)
         for key, good in (("warp_cap", 8), ("cta_set_words", 64), ("cta_set_words", 0),
-                          ("stage_wait_polls", 0), ("min_blocks", 3), ("src_block_bytes", 1 << 20),
-                          ("src_block_bytes", 0)):
+                          ("stage_wait_polls", 0), ("min_blocks", 3)):
             assert L.gary_tune(key.encode(), good) == _lib.GARY_OK, (key, good)
     finally:
         assert L.gary_tune(b"reset", 0) == _lib.GARY_OK

@@ -246,8 +246,7 @@ def test_rmat18_vs_oracle(cuda):
     {"warp_tile_cost": 1 << 12, "cta_tile_cost": 1 << 16, "min_blocks": 3},
     {"warp_tile_cost": 1 << 18, "cta_tile_cost": 1 << 23, "min_blocks": 2},
     {"warp_tile_cost": 1 << 15, "cta_tile_cost": 1 << 20, "vertex_overhead": 0, "min_blocks": 2},
-    {"src_block_bytes": 1 << 20},
-    {"src_block_bytes": 1 << 20, "warp_cap": 8, "cta_set_words": 64, "warp_tile_cost": 1 << 11},
+    {"warp_cap": 8, "cta_set_words": 64, "warp_tile_cost": 1 << 11},
 ])
 def test_tile_shapes_keep_the_count(cuda, cfg):
     """The scheduler's tile shapes change only how work is cut, never the count."""
@@ -323,32 +322,3 @@ def test_block_cache_reuse_across_shapes(cuda):
     for g in again:
         g.free()
 
-
-def test_source_blocks_keep_counts_and_shards(cuda):
-    """Cutting the plan into source blocks (1 MiB of lists each: about ten
-    blocks on RMAT-17) changes only the order of the work: the count and the
-    shard sums stay exact, and every launch reports a clean status."""
-    import torch
-
-    from gary_b200 import autotune
-
-    n = 1 << 17
-    src, dst = gb.gen_rmat(17, 8, 16 << 17)
-    ptr, idx = gb.csr_from_edges(src, dst, n)
-    optr, oidx = O.orient(ptr, idx)
-    want = O.tri_count(optr, oidx)
-    try:
-        for blk in (1 << 20, 3 << 20, 0):
-            autotune.apply({"src_block_bytes": blk})
-            with _upload_host(ptr, idx, n) as g:
-                assert g.count() == want, blk
-                out = torch.zeros(1, dtype=torch.int64, device="cuda")
-                total = 0
-                for sh in range(3):
-                    _lib.check(_lib.load().gary_count_shard_async(g.handle, 3, 0, sh, 3, None, out.data_ptr()),
-                               "shard")
-                    assert g.status() == _lib.GARY_OK
-                    total += int(out.item())
-                assert total == want, blk
-    finally:
-        autotune.apply({})
