@@ -9,8 +9,14 @@ intersectSmall's cg::memcpy_async, include/ops/Intersection.cuh:142-164).  On
 the bench graphs only the first two occur: the last two need d+(v) > 8192
 with an id span beyond 2^19.  The test-only tuning keys "warp_cap" and
 "cta_set_words" send small RMAT graphs down every path, and the per-path tile
-counts in gary_count_last_stats prove each one ran.  Counts are bit-exact
-against the CPU oracle.
+counts in gary_count_last_stats prove each one ran.  The graph that reaches
+them is an Erdos-Renyi graph of 2^17 vertices and average degree 96: ranks by
+degree put most out-neighbour lists across more than 32 K ids (too wide for
+a warp bitmap), with out-degrees from a few to over 100, so with warp_cap 8
+and 64 shared words per CTA set the CTA tiles split between buckets
+(d+ <= 32), staged lists (<= 64) and samples (beyond).  RMAT graphs of this
+size have no such vertices: their wide lists are short.  Counts are
+bit-exact against the CPU oracle.
 
 The bounded waits: "stage_wait_polls" = 0 makes the first wait for every
 staging copy give up at once.  The launch must then report GARY_ERR_TIMEOUT
@@ -53,6 +59,14 @@ def _rmat(scale, ef, seed):
     return n, ptr, idx, O.tri_count(optr, oidx)
 
 
+def _er_wide():
+    n = 1 << 17
+    src, dst = gb.gen_er(n, n * 48, 7)
+    ptr, idx = O.sym_csr(src, dst, n)
+    optr, oidx = O.orient(ptr, idx)
+    return n, ptr, idx, O.tri_count(optr, oidx)
+
+
 def _count_with(g, **kv):
     """Count after rebuilding the plan under the given knobs; (count, stats)."""
     _lib.check(_lib.load().gary_graph_drop_plans(g.handle), "drop plans")
@@ -62,9 +76,8 @@ def _count_with(g, **kv):
     return c, g.last_stats()
 
 
-@pytest.mark.parametrize("scale,ef,seed", [(16, 16, 5), (18, 16, 11)])
-def test_every_cta_set_path_runs_and_counts_exactly(cuda, scale, ef, seed):
-    n, ptr, idx, want = _rmat(scale, ef, seed)
+def test_every_cta_set_path_runs_and_counts_exactly(cuda):
+    n, ptr, idx, want = _er_wide()
     try:
         with gb.Graph.upload(ptr, idx, n) as g:
             plain = g.count()
@@ -79,7 +92,7 @@ def test_every_cta_set_path_runs_and_counts_exactly(cuda, scale, ef, seed):
             p = st["cta_path_tiles"]
             assert p["buckets"] > 0 and p["staged"] > 0 and p["sampled"] > 0, st
             assert sum(p.values()) == st["cta_tiles"]
-            # a mid-sized buffer mixes all four
+            # a mid-sized buffer mixes the paths
             c, st = _count_with(g, warp_cap=16, cta_set_words=256)
             assert c == want and st["error"] == 0
             assert sum(st["cta_path_tiles"].values()) == st["cta_tiles"]
@@ -87,10 +100,24 @@ def test_every_cta_set_path_runs_and_counts_exactly(cuda, scale, ef, seed):
         _reset()
 
 
+@pytest.mark.parametrize("scale,ef,seed", [(16, 16, 5), (18, 16, 11)])
+def test_small_cta_sets_keep_rmat_counts(cuda, scale, ef, seed):
+    """The same knobs on RMAT graphs (whatever paths their CTA tiles take)."""
+    n, ptr, idx, want = _rmat(scale, ef, seed)
+    try:
+        with gb.Graph.upload(ptr, idx, n) as g:
+            for kv in ({"warp_cap": 8}, {"warp_cap": 8, "cta_set_words": 64}, {"warp_cap": 16, "cta_set_words": 256}):
+                c, st = _count_with(g, **kv)
+                assert c == want and st["error"] == 0, kv
+                assert sum(st["cta_path_tiles"].values()) == st["cta_tiles"], kv
+    finally:
+        _reset()
+
+
 def test_expired_staging_wait_is_reported_everywhere(cuda):
     import torch
 
-    n, ptr, idx, want = _rmat(16, 16, 5)
+    n, ptr, idx, want = _er_wide()
     L = _lib.load()
     try:
         with gb.Graph.upload(ptr, idx, n) as g:
