@@ -19,11 +19,13 @@
 // Work is cut into tiles of bounded probe count over the in-edge index and
 // served by a persistent scheduler: CTA tiles (large N+(v)) first, then warp
 // tiles.
+#include <cub/cub.cuh>
 #include <thrust/binary_search.h>
 #include <thrust/copy.h>
 #include <thrust/execution_policy.h>
 #include <thrust/fill.h>
 #include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/reverse_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
 #include <thrust/reduce.h>
 #include <thrust/scan.h>
@@ -54,62 +56,77 @@ inline unsigned grid_for(uint64_t items) {
 
 __host__ __device__ __forceinline__ uint64_t min_u64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
-// The in-edge index is the transpose of the DAG: for every oriented edge
-// u -> v whose suffix S(u,v) (the part of N+(u) after v) is non-empty, and
-// with d+(v) > 0, one record {first word of S(u,v), |S(u,v)|} in v's group.
-// Built without a sort: a count pass gives each record its slot in its
-// target's group (the old value of an atomic counter), a scan turns the
-// counts into group offsets, and a fill pass writes every record to its
-// place.  Both passes walk the rows of 32 consecutive vertices per warp,
-// flattened across the lanes (rows are short on average), so adj is read in
-// order.  Within a group the records come in no particular order; the count
-// does not depend on it.
-template <typename F>
-__device__ __forceinline__ void walk_records(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
-                                             uint32_t n, F f) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c * 32 < n; c += nwarps) {
-    const uint64_t u = c * 32 + lane;
-    const uint2 r = u < n ? row[u] : make_uint2(0, 0);
-    const uint32_t incl = warp_inclusive_sum(r.y, lane);
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    for (uint32_t pb = 0; pb < total; pb += 32) {
-      const uint32_t p = pb + lane;
-      const int o = warp_owner(incl, p);
-      const uint32_t ox = __shfl_sync(kFull, incl - r.y, o);
-      const uint32_t base4 = __shfl_sync(kFull, r.x, o);
-      const uint32_t len = __shfl_sync(kFull, r.y, o);
-      if (p < total) {
-        const uint32_t pos = p - ox;
-        const uint32_t rem = len - pos - 1;
-        const uint64_t w = (uint64_t)base4 * 4 + pos;
-        const uint32_t v = adj[w];
-        if (rem && row[v].y) f(w, v, rem);
-      }
+// The in-edge index: for every oriented edge u -> v whose suffix S(u,v) (the
+// part of N+(u) after v) is non-empty, and with d+(v) > 0, one record
+// {first word of S(u,v), |S(u,v)|} in v's group, records in word order.
+// One 8-byte key per padded word w: target << 32 | w for a word that makes a
+// record, (n - 1) << 32 | w for the others (in rank ids the top vertex has no
+// higher neighbour, so no record ever targets it).  A radix sort of the
+// target bits (stable, so w stays ascending within a group) brings the
+// records to the front, grouped; the suffix length is recomputed from w.
+__global__ void k_in_keys(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
+                          const uint32_t *__restrict__ rowid, uint64_t words, uint32_t n,
+                          uint64_t *__restrict__ keys) {
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    const uint2 r = row[rowid[w]];
+    const uint64_t pos = w - (uint64_t)r.x * 4;
+    uint64_t key = (uint64_t)(n - 1) << 32 | w;
+    if (pos + 1 < r.y) {  // a real id with a non-empty suffix
+      const uint32_t v = adj[w];
+      if (row[v].y) key = (uint64_t)v << 32 | w;
     }
+    keys[w] = key;
   }
 }
 
-__global__ void k_in_count(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj, uint32_t n,
-                           uint32_t *__restrict__ cnt, unsigned long long *__restrict__ work,
-                           uint32_t *__restrict__ slot) {
-  walk_records(row, adj, n, [&](uint64_t w, uint32_t v, uint32_t rem) {
-    slot[w] = atomicAdd(&cnt[v], 1u);
-    atomicAdd(&work[v], (unsigned long long)rem);
-  });
+// first index i with keys[i] >> 32 >= x in a sorted array (one thread)
+__global__ void k_first_target(const uint64_t *__restrict__ keys, uint64_t len, uint32_t x,
+                               uint64_t *__restrict__ out) {
+  uint64_t b = 0, e = len;
+  while (b < e) {
+    const uint64_t m = (b + e) >> 1;
+    if ((uint32_t)(keys[m] >> 32) < x) b = m + 1;
+    else e = m;
+  }
+  *out = b;
 }
 
-__global__ void k_in_fill(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj, uint32_t n,
-                          const uint64_t *__restrict__ inptr, const uint32_t *__restrict__ slot,
-                          uint2 *__restrict__ inedge) {
-  walk_records(row, adj, n, [&](uint64_t w, uint32_t v, uint32_t rem) {
-    inedge[inptr[v] + slot[w]] = make_uint2((uint32_t)(w + 1), rem);
-  });
+// Records from the sorted keys, the group heads (inptr[v] = first record of
+// v), and work[v] = sum of v's suffix lengths (a segmented warp sum, one
+// atomic per run of equal targets).
+__global__ void k_in_records(const uint64_t *__restrict__ keys, uint64_t m, const uint2 *__restrict__ row,
+                             const uint32_t *__restrict__ rowid, uint2 *__restrict__ inedge,
+                             uint64_t *__restrict__ inptr, unsigned long long *__restrict__ work) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < m; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    const bool ok = i < m;
+    uint32_t v = 0xFFFFFFFFu;
+    unsigned long long x = 0;
+    if (ok) {
+      const uint64_t k = keys[i];
+      v = (uint32_t)(k >> 32);
+      const uint32_t w = (uint32_t)k;
+      const uint2 r = row[rowid[w]];
+      const uint32_t rem = r.y - (w - r.x * 4) - 1;
+      inedge[i] = make_uint2(w + 1, rem);
+      x = rem;
+      if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != v) inptr[v] = i;
+    }
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long t = __shfl_up_sync(kFull, x, o);
+      const uint32_t tv = __shfl_up_sync(kFull, v, o);
+      if (lane >= o && tv == v) x += t;
+    }
+    const uint32_t nv = __shfl_down_sync(kFull, v, 1);
+    if (ok && (lane == 31 || nv != v) && x) atomicAdd(&work[v], x);
+  }
 }
 
-struct U32ToU64 {
-  __host__ __device__ uint64_t operator()(uint32_t x) const { return x; }
+struct MinU64 {
+  __host__ __device__ uint64_t operator()(uint64_t a, uint64_t b) const { return a < b ? a : b; }
 };
 
 // pcost (optional): predicted cycles of a warp-class vertex, with tile target
@@ -289,29 +306,48 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
   }
   ScratchAlloc pol_alloc{s};
   auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
-  DevBuf<uint32_t> cnt, slot;
-  GARY_TRY(cnt.alloc((uint64_t)n + 1, s));
-  GARY_TRY(slot.alloc(std::max<uint64_t>(W, 1), s));
-  GARY_TRY(in.work.alloc_persistent(n));
-  GARY_CUDA(cudaMemsetAsync(cnt.p, 0, ((uint64_t)n + 1) * 4, s));
-  GARY_CUDA(cudaMemsetAsync(in.work.p, 0, (uint64_t)n * 8, s));
-  const unsigned grid = grid_for((uint64_t)n);  // one warp per 32 rows
-  k_in_count<<<grid, kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, n, cnt.p,
-                                       reinterpret_cast<unsigned long long *>(in.work.p), slot.p);
-  GARY_CUDA(cudaGetLastError());
-  GARY_TRY(in.inptr.alloc_persistent((uint64_t)n + 1));
-  auto wide = thrust::make_transform_iterator(cnt.p, U32ToU64());
-  thrust::exclusive_scan(pol, wide, wide + n + 1, in.inptr.p, 0ull);
-  uint64_t m = 0;
-  GARY_CUDA(cudaMemcpyAsync(&m, in.inptr.p + n, 8, cudaMemcpyDeviceToHost, s));
-  GARY_CUDA(cudaStreamSynchronize(s));
-  cnt.release();
-  in.records = m;
-  GARY_TRY(in.inedge.alloc_persistent(std::max<uint64_t>(m, 1)));
-  if (m) {
-    k_in_fill<<<grid, kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, n, in.inptr.p, slot.p, in.inedge.p);
+  DevBuf<uint32_t> rowid;
+  DevBuf<uint64_t> keys, keys2;
+  GARY_TRY(padded_rowid(g->dag, rowid, s));
+  GARY_TRY(keys.alloc(std::max<uint64_t>(W, 1), s));
+  GARY_TRY(keys2.alloc(std::max<uint64_t>(W, 1), s));
+  if (W) {
+    k_in_keys<<<grid_for(W), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, rowid.p, W, n, keys.p);
     GARY_CUDA(cudaGetLastError());
+    cub::DoubleBuffer<uint64_t> kb(keys.p, keys2.p);
+    size_t tmp = 0;
+    int eb = 1;  // targets <= n - 1
+    while (eb < 32 && ((uint64_t)n - 1) >> eb) ++eb;
+    GARY_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, kb, W, 32, 32 + eb, s));
+    DevBuf<uint8_t> t;
+    GARY_TRY(t.alloc(std::max<size_t>(tmp, 1), s));
+    GARY_CUDA(cub::DeviceRadixSort::SortKeys(t.p, tmp, kb, W, 32, 32 + eb, s));
+    if (kb.Current() != keys.p) std::swap(keys, keys2);
   }
+  keys2.release();
+  // records = keys whose target is below n - 1
+  uint64_t m = 0;
+  if (W) {
+    DevBuf<uint64_t> pos;
+    GARY_TRY(pos.alloc(1, s));
+    k_first_target<<<1, 1, 0, s>>>(keys.p, W, n - 1, pos.p);
+    GARY_CUDA(cudaGetLastError());
+    GARY_CUDA(cudaMemcpyAsync(&m, pos.p, 8, cudaMemcpyDeviceToHost, s));
+    GARY_CUDA(cudaStreamSynchronize(s));
+  }
+  in.records = m;
+  GARY_TRY(in.inptr.alloc_persistent((uint64_t)n + 1));
+  GARY_TRY(in.inedge.alloc_persistent(std::max<uint64_t>(m, 1)));
+  GARY_TRY(in.work.alloc_persistent(n));
+  thrust::fill(pol, in.inptr.p, in.inptr.p + n + 1, m);
+  GARY_CUDA(cudaMemsetAsync(in.work.p, 0, (uint64_t)n * 8, s));
+  if (m)
+    k_in_records<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, g->dag.row.p, rowid.p, in.inedge.p, in.inptr.p,
+                                                  reinterpret_cast<unsigned long long *>(in.work.p));
+  GARY_CUDA(cudaGetLastError());
+  // vertices without records start where the next group starts
+  auto rb = thrust::make_reverse_iterator(in.inptr.p + n + 1);
+  thrust::inclusive_scan(pol, rb, rb + n + 1, rb, MinU64());
   in.total_work = thrust::reduce(pol, in.work.p, in.work.p + n, 0ull);
   return GARY_OK;
 }
@@ -464,10 +500,22 @@ __device__ __forceinline__ uint32_t walk_chunk(const uint4 *__restrict__ adj4,
   const uint32_t total = __shfl_sync(kFull, incl, 31);
   if (total == 0) return 0;
   // flattened position p of record k's octets maps to octet (o0 - excl) + p
-  const uint32_t bias = o0 - (incl - no);
+  const uint32_t excl = incl - no;
+  const uint32_t bias = o0 - excl;
+  const uint32_t below = (1u << lane) - 1u;
+  // The record owning position pb + lane: `base` owns pb, and every record
+  // that starts in (pb, pb + lane] moves it one on.  Each record sets the bit
+  // of its start inside the batch window (pb, pb + 32]; one OR across the
+  // warp gives all of them.  Only records past the last one have no
+  // octets, and they start at `total`, which no loaded position reaches.
+  uint32_t base = 0;
   auto fetch = [&](uint32_t pb, uint4 &a, uint4 &b) {
+    const uint32_t d = excl - pb - 1u;
+    const uint32_t starts = __reduce_or_sync(kFull, d < 32u ? 1u << d : 0u);
+    const uint32_t own = base + __popc(starts & below);
+    base += __popc(starts);
     const uint32_t p = pb + lane;
-    const uint32_t oc = __shfl_sync(kFull, bias, warp_owner(incl, p)) + p;
+    const uint32_t oc = __shfl_sync(kFull, bias, own) + p;
     if (p < total) {
       a = adj4[2 * oc];
       b = adj4[2 * oc + 1];
