@@ -54,67 +54,76 @@ inline unsigned grid_for(uint64_t items) {
   return (unsigned)std::max<uint64_t>(std::min(b, cap), 1);
 }
 
+inline int bits_for(uint64_t x) {
+  int b = 0;
+  while (b < 64 && (x - 1) >> b) ++b;
+  return std::max(b, 1);
+}
+
 __host__ __device__ __forceinline__ uint64_t min_u64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
-// The in-edge index: for every oriented edge u -> v whose suffix S(u,v) (the
-// part of N+(u) after v) is non-empty, and with d+(v) > 0, one record
-// {first word of S(u,v), |S(u,v)|} in v's group, records in word order.
-// One 8-byte key per padded word w: target << 32 | w for a word that makes a
-// record, (n - 1) << 32 | w for the others (in rank ids the top vertex has no
-// higher neighbour, so no record ever targets it).  A radix sort of the
-// target bits (stable, so w stays ascending within a group) brings the
-// records to the front, grouped; the suffix length is recomputed from w.
-__global__ void k_in_keys(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
-                          const uint32_t *__restrict__ rowid, uint64_t words, uint32_t n,
-                          uint64_t *__restrict__ keys) {
+struct MinU64 {
+  __host__ __device__ uint64_t operator()(uint64_t a, uint64_t b) const { return a < b ? a : b; }
+};
+
+// One candidate per padded word w of N+(u): the suffix after v = adj[w].
+// Words without a record get the key n - 1: in rank ids the top vertex has
+// no higher neighbour, so no record ever targets it, and the keys of an
+// n = 2^k graph fit k bits (one radix pass fewer than with the key n).
+__global__ void k_in_candidates(const uint2 *__restrict__ row, const uint32_t *__restrict__ adj,
+                                const uint32_t *__restrict__ rowid, uint64_t words, uint32_t n,
+                                uint32_t *__restrict__ keys, uint2 *__restrict__ vals) {
   for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < words;
        w += (uint64_t)gridDim.x * blockDim.x) {
-    const uint2 r = row[rowid[w]];
+    const uint32_t u = rowid[w];
+    const uint2 r = row[u];
     const uint64_t pos = w - (uint64_t)r.x * 4;
-    uint64_t key = (uint64_t)(n - 1) << 32 | w;
-    if (pos + 1 < r.y) {  // a real id with a non-empty suffix
+    uint32_t key = n - 1;
+    uint2 val = make_uint2(0, 0);
+    if (pos < r.y) {
       const uint32_t v = adj[w];
-      if (row[v].y) key = (uint64_t)v << 32 | w;
+      const uint32_t rem = r.y - (uint32_t)pos - 1;
+      if (rem && row[v].y) {
+        key = v;
+        val = make_uint2((uint32_t)(w + 1), rem);
+      }
     }
     keys[w] = key;
+    vals[w] = val;
   }
 }
 
-// first index i with keys[i] >> 32 >= x in a sorted array (one thread)
-__global__ void k_first_target(const uint64_t *__restrict__ keys, uint64_t len, uint32_t x,
-                               uint64_t *__restrict__ out) {
+// first index i with keys[i] >= x in a sorted array (one thread)
+__global__ void k_first_geq(const uint32_t *__restrict__ keys, uint64_t len, uint32_t x,
+                            uint64_t *__restrict__ out) {
   uint64_t b = 0, e = len;
   while (b < e) {
     const uint64_t m = (b + e) >> 1;
-    if ((uint32_t)(keys[m] >> 32) < x) b = m + 1;
+    if (keys[m] < x) b = m + 1;
     else e = m;
   }
   *out = b;
 }
 
-// Records from the sorted keys, the group heads (inptr[v] = first record of
-// v), and work[v] = sum of v's suffix lengths (a segmented warp sum, one
-// atomic per run of equal targets).
-__global__ void k_in_records(const uint64_t *__restrict__ keys, uint64_t m, const uint2 *__restrict__ row,
-                             const uint32_t *__restrict__ rowid, uint2 *__restrict__ inedge,
-                             uint64_t *__restrict__ inptr, unsigned long long *__restrict__ work) {
+__global__ void k_in_heads(const uint32_t *__restrict__ keys, uint64_t m,
+                           uint64_t *__restrict__ inptr) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t v = keys[i];
+    if (i == 0 || keys[i - 1] != v) inptr[v] = i;
+  }
+}
+
+// work[v] = sum of suffix lengths of v's in-edges (segmented warp scan; keys sorted).
+__global__ void k_in_work(const uint32_t *__restrict__ keys, const uint2 *__restrict__ vals,
+                          uint64_t m, unsigned long long *__restrict__ work) {
   const int lane = threadIdx.x & 31;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x; base < m; base += stride) {
     const uint64_t i = base + threadIdx.x;
     const bool ok = i < m;
-    uint32_t v = 0xFFFFFFFFu;
-    unsigned long long x = 0;
-    if (ok) {
-      const uint64_t k = keys[i];
-      v = (uint32_t)(k >> 32);
-      const uint32_t w = (uint32_t)k;
-      const uint2 r = row[rowid[w]];
-      const uint32_t rem = r.y - (w - r.x * 4) - 1;
-      inedge[i] = make_uint2(w + 1, rem);
-      x = rem;
-      if (i == 0 || (uint32_t)(keys[i - 1] >> 32) != v) inptr[v] = i;
-    }
+    const uint32_t v = ok ? keys[i] : 0xFFFFFFFFu;
+    unsigned long long x = ok ? vals[i].y : 0ull;
     for (int o = 1; o < 32; o <<= 1) {
       const unsigned long long t = __shfl_up_sync(kFull, x, o);
       const uint32_t tv = __shfl_up_sync(kFull, v, o);
@@ -124,10 +133,6 @@ __global__ void k_in_records(const uint64_t *__restrict__ keys, uint64_t m, cons
     if (ok && (lane == 31 || nv != v) && x) atomicAdd(&work[v], x);
   }
 }
-
-struct MinU64 {
-  __host__ __device__ uint64_t operator()(uint64_t a, uint64_t b) const { return a < b ? a : b; }
-};
 
 // pcost (optional): predicted cycles of a warp-class vertex, with tile target
 // tw_pred in the same unit; without it, costs are probe counts.
@@ -153,7 +158,11 @@ __global__ void k_classify(const uint2 *__restrict__ row, const uint32_t *__rest
       const bool warp_fits = bitmap || dv <= pp.warp_cap;
       const uint64_t build = bitmap ? (span >> 5) + dv : 4ull * dv;
       const bool pred = pcost && warp_fits;
-      const uint64_t c = pred ? pcost[v] + 1 : work[v] + build + pp.vertex_overhead;
+      const uint64_t cp = work[v] + build + pp.vertex_overhead;  // probe cost
+      // learned: predicted cycles, but never below the probe cost scaled to
+      // the same tile target, so that no tile outgrows a plain one (a vertex
+      // the model under-rates would otherwise end the launch alone)
+      const uint64_t c = pred ? max(pcost[v] + 1, cp * tw_pred / pp.warp_tile_cost) : cp;
       const uint64_t tw = pred ? tw_pred : pp.warp_tile_cost;
       if (!warp_fits) {
         cls = kClassCta;
@@ -306,48 +315,58 @@ int build_in_index(gary_graph *g, cudaStream_t s, InIndex &in) {
   }
   ScratchAlloc pol_alloc{s};
   auto pol = thrust::cuda::par_nosync(pol_alloc).on(s);
-  DevBuf<uint32_t> rowid;
-  DevBuf<uint64_t> keys, keys2;
-  GARY_TRY(padded_rowid(g->dag, rowid, s));
-  GARY_TRY(keys.alloc(std::max<uint64_t>(W, 1), s));
-  GARY_TRY(keys2.alloc(std::max<uint64_t>(W, 1), s));
-  if (W) {
-    k_in_keys<<<grid_for(W), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, rowid.p, W, n, keys.p);
+  DevBuf<uint32_t> keys, keys2;
+  DevBuf<uint2> vals, vals2;
+  {
+    DevBuf<uint32_t> rowid;
+    GARY_TRY(padded_rowid(g->dag, rowid, s));
+    GARY_TRY(keys.alloc(W, s));
+    GARY_TRY(vals.alloc(W, s));
+    k_in_candidates<<<grid_for(W), kThreads, 0, s>>>(g->dag.row.p, g->dag.adj.p, rowid.p, W, n, keys.p,
+                                                     vals.p);
     GARY_CUDA(cudaGetLastError());
-    cub::DoubleBuffer<uint64_t> kb(keys.p, keys2.p);
+  }
+  GARY_TRY(keys2.alloc(W, s));
+  GARY_TRY(vals2.alloc(W, s));
+  {
+    cub::DoubleBuffer<uint32_t> kb(keys.p, keys2.p);
+    cub::DoubleBuffer<uint2> vb(vals.p, vals2.p);
     size_t tmp = 0;
-    int eb = 1;  // targets <= n - 1
-    while (eb < 32 && ((uint64_t)n - 1) >> eb) ++eb;
-    GARY_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp, kb, W, 32, 32 + eb, s));
+    const int eb = bits_for((uint64_t)n);  // keys <= n - 1
+    GARY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, kb, vb, W, 0, eb, s));
     DevBuf<uint8_t> t;
-    GARY_TRY(t.alloc(std::max<size_t>(tmp, 1), s));
-    GARY_CUDA(cub::DeviceRadixSort::SortKeys(t.p, tmp, kb, W, 32, 32 + eb, s));
+    GARY_TRY(t.alloc(tmp, s));
+    GARY_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, kb, vb, W, 0, eb, s));
     if (kb.Current() != keys.p) std::swap(keys, keys2);
+    if (vb.Current() != vals.p) std::swap(vals, vals2);
   }
   keys2.release();
-  // records = keys whose target is below n - 1
+  vals2.release();
+  // records = number of keys < n - 1 (the rest carry the "no record" key n - 1)
   uint64_t m = 0;
-  if (W) {
+  {
     DevBuf<uint64_t> pos;
     GARY_TRY(pos.alloc(1, s));
-    k_first_target<<<1, 1, 0, s>>>(keys.p, W, n - 1, pos.p);
+    k_first_geq<<<1, 1, 0, s>>>(keys.p, W, n - 1, pos.p);
     GARY_CUDA(cudaGetLastError());
     GARY_CUDA(cudaMemcpyAsync(&m, pos.p, 8, cudaMemcpyDeviceToHost, s));
     GARY_CUDA(cudaStreamSynchronize(s));
   }
   in.records = m;
   GARY_TRY(in.inptr.alloc_persistent((uint64_t)n + 1));
-  GARY_TRY(in.inedge.alloc_persistent(std::max<uint64_t>(m, 1)));
-  GARY_TRY(in.work.alloc_persistent(n));
   thrust::fill(pol, in.inptr.p, in.inptr.p + n + 1, m);
-  GARY_CUDA(cudaMemsetAsync(in.work.p, 0, (uint64_t)n * 8, s));
-  if (m)
-    k_in_records<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, g->dag.row.p, rowid.p, in.inedge.p, in.inptr.p,
-                                                  reinterpret_cast<unsigned long long *>(in.work.p));
-  GARY_CUDA(cudaGetLastError());
-  // vertices without records start where the next group starts
+  if (m) k_in_heads<<<grid_for(m), kThreads, 0, s>>>(keys.p, m, in.inptr.p);
   auto rb = thrust::make_reverse_iterator(in.inptr.p + n + 1);
   thrust::inclusive_scan(pol, rb, rb + n + 1, rb, MinU64());
+  GARY_TRY(in.inedge.alloc_persistent(std::max<uint64_t>(m, 1)));
+  if (m)
+    GARY_CUDA(cudaMemcpyAsync(in.inedge.p, vals.p, m * sizeof(uint2), cudaMemcpyDeviceToDevice, s));
+  GARY_TRY(in.work.alloc_persistent(n));
+  GARY_CUDA(cudaMemsetAsync(in.work.p, 0, (uint64_t)n * 8, s));
+  if (m)
+    k_in_work<<<grid_for(m), kThreads, 0, s>>>(keys.p, vals.p, m,
+                                              reinterpret_cast<unsigned long long *>(in.work.p));
+  GARY_CUDA(cudaGetLastError());
   in.total_work = thrust::reduce(pol, in.work.p, in.work.p + n, 0ull);
   return GARY_OK;
 }
