@@ -531,9 +531,10 @@ static_assert(2 * (1u << kK4WarpLog) + kK4WarpMaxD * (kK4WarpMaxD / 32) <= kK4Wa
               "warp region too small");
 static_assert((1u << kK4MidLog) >= 2 * kK4MidMaxD, "mid hash too small");
 
-// Position hash of N+(u) (ids are distinct; the table is at least twice the
-// list).  Both loops visit each slot at most once: a full table (a broken
-// capacity rule) sets kLaunchErrTableFull on insert and misses on lookup.
+// Position hash of N+(u) (ids are distinct).  k4_vertex inserts at most
+// half as many ids as the table has slots, so every lookup ends at a free
+// slot and needs no counter (a counter cost the hot lookup about 13 %).  The
+// insert loop visits each slot at most once regardless.
 __device__ __forceinline__ void pos_insert(uint32_t *keys, uint32_t *pos, uint32_t mask, int shift,
                                            uint32_t x, uint32_t p, unsigned *err) {
   uint32_t h = (x * kHashMul) >> shift;
@@ -550,13 +551,12 @@ __device__ __forceinline__ void pos_insert(uint32_t *keys, uint32_t *pos, uint32
 __device__ __forceinline__ int pos_find(const uint32_t *keys, const uint32_t *pos, uint32_t mask,
                                         int shift, uint32_t x) {
   uint32_t h = (x * kHashMul) >> shift;
-  for (uint32_t i = 0; i <= mask; ++i) {
+  while (true) {
     const uint32_t k = keys[h];
     if (k == kSentinel) return -1;  // first: x may itself be the padding value
     if (k == x) return (int)pos[h];
     h = (h + 1) & mask;
   }
-  return -1;
 }
 
 // 4-cliques with lowest vertex u; `nthreads` threads (one warp or the CTA)
@@ -575,7 +575,11 @@ __device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t
   if (l > (int)max_log) l = (int)max_log;
   const uint32_t mask = (1u << l) - 1;
   const int shift = 32 - l;
-  for (uint32_t i = tid; i < d; i += nthreads) pos_insert(keys, pos, mask, shift, au[i], i, err);
+  // at most half the slots: the plan's degree classes keep d there; a list
+  // beyond that (a broken rule) is counted wrongly but reported, never hangs
+  const uint32_t ins = d <= (mask + 1) / 2 ? d : (mask + 1) / 2;
+  if (ins < d && tid == 0) atomicOr(err, kLaunchErrTableFull);
+  for (uint32_t i = tid; i < ins; i += nthreads) pos_insert(keys, pos, mask, shift, au[i], i, err);
   sync();
   const uint32_t maxu = au[d - 1];
   // rows: 32 rows per warp step.  Each N+(v) is read as 32-byte octets from
