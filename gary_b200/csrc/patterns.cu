@@ -320,7 +320,10 @@ __device__ __forceinline__ uint32_t warp_min_u32(uint32_t x) {
 }
 
 // Walk, for the 32 list ranges [b_k, e_k) of the lanes' v's, every id w of
-// N(v_k) in that range (flattened across the lanes); call f(w).  All lanes call.
+// N(v_k) in that range (flattened across the lanes); call f(w).  All lanes
+// call.  The ranges of the active neighbours are never empty (each has an id
+// in the window) and the lanes past the active list come last, so the owners
+// follow from the starts (WarpOwners).
 template <typename F>
 __device__ __forceinline__ void walk_ranges(const uint32_t *__restrict__ adj, uint32_t q4, uint32_t b,
                                             uint32_t e, int lane, F f) {
@@ -328,9 +331,10 @@ __device__ __forceinline__ void walk_ranges(const uint32_t *__restrict__ adj, ui
   const uint32_t incl = warp_inclusive_sum(len, lane);
   const uint32_t total = __shfl_sync(kFull, incl, 31);
   const uint32_t shift = b - (incl - len);  // word of flattened position p: q4*4 + shift + p
+  WarpOwners own(incl - len, lane);
   for (uint32_t pb = 0; pb < total; pb += 32) {
     const uint32_t p = pb + lane;
-    const int o = warp_owner(incl, p);
+    const int o = (int)own.owner(pb);
     const uint32_t oq = __shfl_sync(kFull, q4, o);
     const uint32_t os = __shfl_sync(kFull, shift, o);
     if (p < total) f(adj[(uint64_t)oq * 4 + (uint32_t)(os + p)]);

@@ -40,6 +40,27 @@ __device__ __forceinline__ int warp_owner(uint32_t incl, uint32_t p) {
   return lo;
 }
 
+// The owners of a flattened walk's positions, batch after batch: segment k
+// (lane k's) covers [excl_k, excl_k + len_k) of the concatenation, and the
+// walk visits positions pb + lane for pb = 0, 32, 64, ... in order.  Every
+// segment sets the bit of its start inside (pb, pb + 32]; one OR across the
+// warp gives all of them, and the owner of pb + lane is the owner of pb moved
+// on by the starts at or before it.  Precondition: no empty segment before
+// the last non-empty one (trailing empty segments start at the total, which
+// no position reaches).  All 32 lanes must call owner() for every batch.
+struct WarpOwners {
+  uint32_t excl, below, base;
+  __device__ __forceinline__ WarpOwners(uint32_t excl_, int lane)
+      : excl(excl_), below((1u << lane) - 1u), base(0) {}
+  __device__ __forceinline__ uint32_t owner(uint32_t pb) {
+    const uint32_t d = excl - pb - 1u;
+    const uint32_t starts = __reduce_or_sync(kFull, d < 32u ? 1u << d : 0u);
+    const uint32_t own = base + __popc(starts & below);
+    base += __popc(starts);
+    return own;
+  }
+};
+
 __device__ __forceinline__ uint32_t warp_inclusive_sum(uint32_t x, int lane) {
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
