@@ -191,21 +191,24 @@ def workload_config(args, world: int) -> dict:
 # Sources the triangle kernel is built from: a counter capture stored under
 # profiles/ applies to the build whose sources hash to its "kernel_src".
 KERNEL_SOURCES = ("tc.cu", "tc.cuh", "warp_ops.cuh", "bulk.cuh", "internal.cuh", "graph.cuh")
+# the 4-cycle and 4-clique count kernels
+PATTERN_SOURCES = ("patterns.cu", "patterns.cuh", "warp_ops.cuh", "internal.cuh", "graph.cuh")
 
 
-def kernel_source_hash() -> str:
+def kernel_source_hash(sources=KERNEL_SOURCES) -> str:
     import hashlib
 
     h = hashlib.sha256()
-    for name in KERNEL_SOURCES:
+    for name in sources:
         h.update((ROOT / "gary_b200" / "csrc" / name).read_bytes())
     return h.hexdigest()[:16]
 
 
-def measured_counters(workload: str):
+def measured_counters(workload: str, sources=KERNEL_SOURCES):
     """The ncu counters stored for `workload` (profiles/roofline_traffic.json:
-    DRAM bytes, warp instructions and L2->SM bytes of one launch), with
-    `stale` true when they were captured on other kernel sources."""
+    DRAM bytes, warp instructions and L2->SM bytes of one launch, or of one
+    count call's kernels for the 4-vertex patterns), with `stale` true when
+    they were captured on other kernel sources."""
     f = ROOT / "profiles" / "roofline_traffic.json"
     if not f.exists():
         return None
@@ -216,7 +219,7 @@ def measured_counters(workload: str):
     if not isinstance(rec, dict):
         return None
     rec = dict(rec)
-    rec["stale"] = rec.get("kernel_src") != kernel_source_hash()
+    rec["stale"] = rec.get("kernel_src") != kernel_source_hash(sources)
     return rec
 
 
@@ -798,6 +801,25 @@ def batch_measure(args, steps: int, warmup: int) -> dict:
     return line
 
 
+def pattern_roofline(workload: str, ms: float):
+    """DRAM and issue fractions of one 4-cycle / 4-clique count call: the ncu
+    counters stored for the workload (all the call's count kernels, summed)
+    over the call's live CUDA-event time; None when none are stored."""
+    mc = measured_counters(workload, PATTERN_SOURCES)
+    if not mc:
+        return None
+    hbm, src = peak_hbm()
+    t = ms / 1e3
+    ceiling = sm_count() * 4 * 1965e6  # 4 schedulers per SM at the maximum SM clock
+    return {"bound": "hbm", "achieved": mc["dram_bytes"] / t / 1e9, "peak": hbm, "unit": "GB/s",
+            "frac": mc["dram_bytes"] / t / 1e9 / hbm, "traffic": mc["dram_bytes"], "peak_source": src,
+            "achieved_basis": "ncu DRAM bytes of the call's count kernels over the call's CUDA-event time",
+            "issue": {"warp_inst_per_call": mc["warp_inst"], "ceiling_per_s": ceiling,
+                      "frac": mc["warp_inst"] / t / ceiling},
+            "kernels": mc.get("kernels"), "source": mc.get("profile"), "kernel_src": mc.get("kernel_src"),
+            "stale": mc["stale"]}
+
+
 def run_patterns(args, dist):
     """Triangle, 4-cycle and 4-clique counts of the seeded RMAT graph (one GPU):
     per pattern the first call (plan building included, wall clock) and the
@@ -854,12 +876,13 @@ def run_patterns(args, dist):
         ocnt = oracle()
         cpu_s = time.perf_counter() - t0
         assert ocnt == scnt, f"{names[pat]}: oracle {ocnt} != GPU {scnt} on the small graph"
+        workload = f"{names[pat]} count, RMAT scale {args.scale} edge factor {args.ef}, seed {args.seed}"
         print(json.dumps({"metric": f"{names[pat]} count time", "value": ms, "unit": "ms", "higher_is_better": False,
                           "pattern": names[pat], "count": cnt, "first_call_s": first_s,
                           "oriented_edges_per_s": m / (ms / 1e3),
                           "steps": args.steps, "warmup": args.warmup, "n_gpus": 1, "data": "synthetic",
-                          "config": {"workload": f"{names[pat]} count, RMAT scale {args.scale} edge factor "
-                                                 f"{args.ef}, seed {args.seed}"},
+                          "config": {"workload": workload},
+                          "roofline": pattern_roofline(workload, ms),
                           "small_graph": {"workload": f"RMAT scale {args.cpu_scale} edge factor {args.ef}",
                                           "gpu_ms": sms, "count": scnt,
                                           "cpu_baseline": {"value": cpu_s * 1e3, "unit": "ms", "kind": "port",
