@@ -105,9 +105,10 @@ __device__ __forceinline__ void c4_wedges(const GraphView &s, const uint32_t *__
     const uint32_t incl = warp_inclusive_sum(len, lane);
     const uint32_t excl = incl - len;
     const uint32_t total = __shfl_sync(kFull, incl, 31);
+    WarpRuns own(excl, len, lane);
     for (uint32_t pb = 0; pb < total; pb += 32) {
       const uint32_t p = pb + lane;
-      const int o = warp_owner(incl, p);
+      const int o = (int)own.owner(pb);
       const uint32_t ox = __shfl_sync(kFull, excl, o);
       const uint32_t ob = __shfl_sync(kFull, base, o);
       if (p < total) f(s.adj[(uint64_t)ob * 4 + (p - ox)]);
@@ -607,9 +608,10 @@ __device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t
     const uint32_t incl = warp_inclusive_sum(no, lane);
     const uint32_t total = __shfl_sync(kFull, incl, 31);
     const uint32_t bias = o0 - (incl - no);
+    WarpRuns own(incl - no, no, lane);
     for (uint32_t pb = 0; pb < total; pb += 32) {
       const uint32_t p = pb + lane;
-      const int o = warp_owner(incl, p);
+      const int o = (int)own.owner(pb);
       const uint32_t oc = __shfl_sync(kFull, bias, o) + p;
       if (p < total) {
         const uint4 a = adj4[2 * (uint64_t)oc], b = adj4[2 * (uint64_t)oc + 1];

@@ -521,18 +521,11 @@ __device__ __forceinline__ uint32_t walk_chunk(const uint4 *__restrict__ adj4,
   // flattened position p of record k's octets maps to octet (o0 - excl) + p
   const uint32_t excl = incl - no;
   const uint32_t bias = o0 - excl;
-  const uint32_t below = (1u << lane) - 1u;
-  // The record owning position pb + lane: `base` owns pb, and every record
-  // that starts in (pb, pb + lane] moves it one on.  Each record sets the bit
-  // of its start inside the batch window (pb, pb + 32]; one OR across the
-  // warp gives all of them.  Only records past the last one have no
-  // octets, and they start at `total`, which no loaded position reaches.
-  uint32_t base = 0;
+  // Every record has octets (a suffix is never empty); only the lanes past
+  // the last record have none, so the owners follow from the record starts.
+  WarpOwners owners(excl, lane);
   auto fetch = [&](uint32_t pb, uint4 &a, uint4 &b) {
-    const uint32_t d = excl - pb - 1u;
-    const uint32_t starts = __reduce_or_sync(kFull, d < 32u ? 1u << d : 0u);
-    const uint32_t own = base + __popc(starts & below);
-    base += __popc(starts);
+    const uint32_t own = owners.owner(pb);
     const uint32_t p = pb + lane;
     const uint32_t oc = __shfl_sync(kFull, bias, own) + p;
     if (p < total) {

@@ -28,18 +28,6 @@ __device__ __forceinline__ int hash_log2(uint32_t items) {
   return l < 5 ? 5 : l;
 }
 
-// Lowest lane index k with incl_k > p, for a non-decreasing per-lane
-// inclusive prefix `incl` (all 32 lanes must call).  5 shuffles.
-__device__ __forceinline__ int warp_owner(uint32_t incl, uint32_t p) {
-  int lo = 0;
-#pragma unroll
-  for (int step = 16; step > 0; step >>= 1) {
-    uint32_t val = __shfl_sync(kFull, incl, lo + step - 1);
-    if (val <= p) lo += step;
-  }
-  return lo;
-}
-
 // The owners of a flattened walk's positions, batch after batch: segment k
 // (lane k's) covers [excl_k, excl_k + len_k) of the concatenation, and the
 // walk visits positions pb + lane for pb = 0, 32, 64, ... in order.  Every
@@ -58,6 +46,40 @@ struct WarpOwners {
     const uint32_t own = base + __popc(starts & below);
     base += __popc(starts);
     return own;
+  }
+};
+
+// Index of the k-th set bit (k from 0) of m, for k < popc(m).
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t k) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t w = 16; w; w >>= 1) {
+    const uint32_t c = __popc((m >> pos) & ((1u << w) - 1u));
+    if (k >= c) {
+      k -= c;
+      pos += w;
+    }
+  }
+  return pos;
+}
+
+// WarpOwners for segments that may be empty anywhere: only non-empty
+// segments set start bits, so the count of starts at or before a position is
+// its owner's rank among the non-empty segments, and lane r holds the lane of
+// the r-th of them.  All 32 lanes must construct and call owner() together.
+struct WarpRuns {
+  uint32_t excl, below, base, lane_of;
+  bool live;
+  __device__ __forceinline__ WarpRuns(uint32_t excl_, uint32_t len, int lane)
+      : excl(excl_), below((1u << lane) - 1u), base(0), live(len != 0) {
+    lane_of = nth_set_bit(__ballot_sync(kFull, live), (uint32_t)lane);
+  }
+  __device__ __forceinline__ uint32_t owner(uint32_t pb) {
+    const uint32_t d = excl - pb - 1u;
+    const uint32_t starts = __reduce_or_sync(kFull, live && d < 32u ? 1u << d : 0u);
+    const uint32_t rank = base + __popc(starts & below);
+    base += __popc(starts);
+    return __shfl_sync(kFull, lane_of, rank);
   }
 };
 
@@ -80,37 +102,6 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x)
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
   return x;
-}
-
-// For the lists N+(v) of v = keys[j], j in the chunks jb, jb+jstep, ... < je
-// (each chunk 32 wide), count the members that `probe(w)` accepts.  The 32
-// lanes walk the concatenation of a chunk's lists, so short lists do not idle
-// lanes.  All 32 lanes must call.  Returns the per-lane count.
-template <typename Probe>
-__device__ __forceinline__ uint32_t warp_walk_lists(const GraphView &g, const uint32_t *keys,
-                                                    uint32_t jb, uint32_t je, uint32_t jstep,
-                                                    int lane, Probe probe) {
-  uint32_t cnt = 0;
-  for (uint32_t j = jb; j < je; j += jstep) {
-    const uint32_t jj = j + lane;
-    uint32_t len = 0, base = 0;
-    if (jj < je) {
-      const uint2 r = g.row[keys[jj]];
-      base = r.x;
-      len = r.y;
-    }
-    const uint32_t incl = warp_inclusive_sum(len, lane);
-    const uint32_t excl = incl - len;
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    for (uint32_t pb = 0; pb < total; pb += 32) {
-      const uint32_t p = pb + lane;
-      const int k = warp_owner(incl, p);
-      const uint32_t ek = __shfl_sync(kFull, excl, k);
-      const uint32_t bk = __shfl_sync(kFull, base, k);
-      if (p < total) cnt += probe(g.adj[(uint64_t)bk * 4 + (p - ek)]);
-    }
-  }
-  return cnt;
 }
 
 // Two-phase search (Search.cuh:120-138 restated): `cache` holds S samples
