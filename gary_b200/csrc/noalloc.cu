@@ -94,9 +94,10 @@ __device__ __forceinline__ uint32_t walk_out_lists(const uint64_t *__restrict__ 
     const uint32_t incl = warp_inclusive_sum(len, lane);
     const uint32_t excl = incl - len;
     const uint32_t total = __shfl_sync(kFull, incl, 31);
+    WarpRuns own(excl, len, lane);
     for (uint32_t pb = 0; pb < total; pb += 32) {
       const uint32_t p = pb + lane;
-      const int o = warp_owner(incl, p);
+      const int o = (int)own.owner(pb);
       const uint32_t ox = __shfl_sync(kFull, excl, o);
       const uint64_t os = __shfl_sync(kFull, start, o);
       if (p < total) cnt += set.contains(colidx[os + (p - ox)]);

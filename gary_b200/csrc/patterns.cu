@@ -105,14 +105,23 @@ __device__ __forceinline__ void c4_wedges(const GraphView &s, const uint32_t *__
     const uint32_t incl = warp_inclusive_sum(len, lane);
     const uint32_t excl = incl - len;
     const uint32_t total = __shfl_sync(kFull, incl, 31);
+    if (total == 0) continue;
     WarpRuns own(excl, len, lane);
-    for (uint32_t pb = 0; pb < total; pb += 32) {
+    // one batch of ids in flight: the next loads while this one is counted
+    auto fetch = [&](uint32_t pb) {
       const uint32_t p = pb + lane;
       const int o = (int)own.owner(pb);
       const uint32_t ox = __shfl_sync(kFull, excl, o);
       const uint32_t ob = __shfl_sync(kFull, base, o);
-      if (p < total) f(s.adj[(uint64_t)ob * 4 + (p - ox)]);
+      return p < total ? s.adj[(uint64_t)ob * 4 + (p - ox)] : kSentinel;
+    };
+    uint32_t cur = fetch(0);
+    for (uint32_t pb = 32; pb < total; pb += 32) {
+      const uint32_t nxt = fetch(pb);
+      f(cur);
+      cur = nxt;
     }
+    if (lane < total - ((total - 1) & ~31u)) f(cur);
   }
 }
 
@@ -333,13 +342,22 @@ __device__ __forceinline__ void walk_ranges(const uint32_t *__restrict__ adj, ui
   const uint32_t total = __shfl_sync(kFull, incl, 31);
   const uint32_t shift = b - (incl - len);  // word of flattened position p: q4*4 + shift + p
   WarpOwners own(incl - len, lane);
-  for (uint32_t pb = 0; pb < total; pb += 32) {
+  // one batch of ids in flight: the next loads while this one is counted
+  auto fetch = [&](uint32_t pb) {
     const uint32_t p = pb + lane;
     const int o = (int)own.owner(pb);
     const uint32_t oq = __shfl_sync(kFull, q4, o);
     const uint32_t os = __shfl_sync(kFull, shift, o);
-    if (p < total) f(adj[(uint64_t)oq * 4 + (uint32_t)(os + p)]);
+    return p < total ? adj[(uint64_t)oq * 4 + (uint32_t)(os + p)] : kSentinel;
+  };
+  if (total == 0) return;
+  uint32_t cur = fetch(0);
+  for (uint32_t pb = 32; pb < total; pb += 32) {
+    const uint32_t nxt = fetch(pb);
+    f(cur);
+    cur = nxt;
   }
+  if (lane < total - ((total - 1) & ~31u)) f(cur);
 }
 
 // Tile {v0 = u, v1 = pre, j0 = wa, j1 = wb}: windows [wa, wb) of vertex u,
