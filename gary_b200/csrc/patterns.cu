@@ -100,28 +100,35 @@ __device__ __forceinline__ void c4_wedges(const GraphView &s, const uint32_t *__
       const uint32_t v = au[k];
       const uint2 rv = s.row[v];
       base = rv.x;
-      len = below_u(s.adj + (uint64_t)rv.x * 4, rv.y, dplus[v], u);
+      len = (below_u(s.adj + (uint64_t)rv.x * 4, rv.y, dplus[v], u) + 3) >> 2;  // quads
     }
     const uint32_t incl = warp_inclusive_sum(len, lane);
     const uint32_t excl = incl - len;
     const uint32_t total = __shfl_sync(kFull, incl, 31);
+    const uint32_t qbase = base - excl;  // quad of flattened position p: qbase + p (mod 2^32) of the owner
     if (total == 0) continue;
     WarpRuns own(excl, len, lane);
-    // one batch of ids in flight: the next loads while this one is counted
+    // one batch of quads in flight: the next loads while this one is counted
+    const uint4 *adj4 = reinterpret_cast<const uint4 *>(s.adj);
     auto fetch = [&](uint32_t pb) {
       const uint32_t p = pb + lane;
       const int o = (int)own.owner(pb);
-      const uint32_t ox = __shfl_sync(kFull, excl, o);
-      const uint32_t ob = __shfl_sync(kFull, base, o);
-      return p < total ? s.adj[(uint64_t)ob * 4 + (p - ox)] : kSentinel;
+      const uint32_t qi = __shfl_sync(kFull, qbase, o) + p;
+      return p < total ? adj4[qi] : make_uint4(kSentinel, kSentinel, kSentinel, kSentinel);
     };
-    uint32_t cur = fetch(0);
+    auto take = [&](const uint4 &a) {
+      if (a.x < u) f(a.x);
+      if (a.y < u) f(a.y);
+      if (a.z < u) f(a.z);
+      if (a.w < u) f(a.w);
+    };
+    uint4 cur = fetch(0);
     for (uint32_t pb = 32; pb < total; pb += 32) {
-      const uint32_t nxt = fetch(pb);
-      f(cur);
+      const uint4 nxt = fetch(pb);
+      take(cur);
       cur = nxt;
     }
-    if (lane < total - ((total - 1) & ~31u)) f(cur);
+    take(cur);
   }
 }
 
@@ -330,34 +337,43 @@ __device__ __forceinline__ uint32_t warp_min_u32(uint32_t x) {
 }
 
 // Walk, for the 32 list ranges [b_k, e_k) of the lanes' v's, every id w of
-// N(v_k) in that range (flattened across the lanes); call f(w).  All lanes
-// call.  The ranges of the active neighbours are never empty (each has an id
-// in the window) and the lanes past the active list come last, so the owners
-// follow from the starts (WarpOwners).
+// N(v_k) in that range; call f(w).  The ranges are read as the 16-byte quads
+// of the (16-byte aligned, sorted, padded) lists that cover them, flattened
+// across the lanes; a quad's other ids lie below lo (before the range) or at
+// or past lo + span (after it, or padding), so the window's own range test
+// rejects them.  All lanes call.  The ranges of the active neighbours are
+// never empty (each has an id in the window) and the lanes past the active
+// list come last, so the owners follow from the starts (WarpOwners).
 template <typename F>
 __device__ __forceinline__ void walk_ranges(const uint32_t *__restrict__ adj, uint32_t q4, uint32_t b,
-                                            uint32_t e, int lane, F f) {
-  const uint32_t len = e - b;
-  const uint32_t incl = warp_inclusive_sum(len, lane);
+                                            uint32_t e, uint32_t lo, uint32_t span, int lane, F f) {
+  const uint32_t nq = e > b ? ((e + 3) >> 2) - (b >> 2) : 0u;
+  const uint32_t incl = warp_inclusive_sum(nq, lane);
   const uint32_t total = __shfl_sync(kFull, incl, 31);
-  const uint32_t shift = b - (incl - len);  // word of flattened position p: q4*4 + shift + p
-  WarpOwners own(incl - len, lane);
-  // one batch of ids in flight: the next loads while this one is counted
+  if (total == 0) return;
+  // quad of flattened position p: qbase + p (mod 2^32) of the owner
+  const uint32_t qbase = q4 + (b >> 2) - (incl - nq);
+  WarpOwners own(incl - nq, lane);
+  const uint4 *adj4 = reinterpret_cast<const uint4 *>(adj);
   auto fetch = [&](uint32_t pb) {
     const uint32_t p = pb + lane;
     const int o = (int)own.owner(pb);
-    const uint32_t oq = __shfl_sync(kFull, q4, o);
-    const uint32_t os = __shfl_sync(kFull, shift, o);
-    return p < total ? adj[(uint64_t)oq * 4 + (uint32_t)(os + p)] : kSentinel;
+    const uint32_t qi = __shfl_sync(kFull, qbase, o) + p;
+    return p < total ? adj4[qi] : make_uint4(kSentinel, kSentinel, kSentinel, kSentinel);
   };
-  if (total == 0) return;
-  uint32_t cur = fetch(0);
+  auto take = [&](const uint4 &a) {
+    if (a.x - lo < span) f(a.x);
+    if (a.y - lo < span) f(a.y);
+    if (a.z - lo < span) f(a.z);
+    if (a.w - lo < span) f(a.w);
+  };
+  uint4 cur = fetch(0);
   for (uint32_t pb = 32; pb < total; pb += 32) {
-    const uint32_t nxt = fetch(pb);
-    f(cur);
+    const uint4 nxt = fetch(pb);
+    take(cur);
     cur = nxt;
   }
-  if (lane < total - ((total - 1) & ~31u)) f(cur);
+  take(cur);
 }
 
 // Tile {v0 = u, v1 = pre, j0 = wa, j1 = wb}: windows [wa, wb) of vertex u,
@@ -499,9 +515,9 @@ __global__ void __launch_bounds__(kWinThreads, 3)
           seen += e - b;
         }
         if (wide)
-          walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { acc += win_incr<true>(cnt, w - lo); });
+          walk_ranges(s.adj, q4, b, e, lo, hi - lo, lane, [&](uint32_t w) { acc += win_incr<true>(cnt, w - lo); });
         else
-          walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { acc += win_incr<false>(cnt, w - lo); });
+          walk_ranges(s.adj, q4, b, e, lo, hi - lo, lane, [&](uint32_t w) { acc += win_incr<false>(cnt, w - lo); });
       }
       nxt = warp_min_u32(nxt);
       seen = warp_sum_u64(seen);
@@ -522,7 +538,7 @@ __global__ void __launch_bounds__(kWinThreads, 3)
             b = cs.prev[k];
             e = cs.cur[k];
           }
-          walk_ranges(s.adj, q4, b, e, lane, [&](uint32_t w) { cnt[wide ? w - lo : (w - lo) >> 1] = 0u; });
+          walk_ranges(s.adj, q4, b, e, lo, hi - lo, lane, [&](uint32_t w) { cnt[wide ? w - lo : (w - lo) >> 1] = 0u; });
         }
       } else {
         for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) cnt[i] = 0;
