@@ -366,7 +366,7 @@ extern "C" int gary_tune(const char *key, uint64_t value) {
   if (k == "warp_tile_cost") p.warp_tile_cost = value;  // 0: from the work
   else if (k == "cta_tile_cost" && value > 0) p.cta_tile_cost = value;
   else if (k == "warp_cap" && value >= 8 && value <= gary::kWarpTableSlots / 2) p.warp_cap = (uint32_t)value;
-  else if (k == "cta_set_words" && (value == 0 || (pow2 && value >= 64 && value <= gary::kTcWarps * gary::kWarpTableSlots)))
+  else if (k == "cta_set_words" && (value == 0 || (pow2 && value >= 64 && value <= gary::kTcMaxWarps * gary::kWarpTableSlots)))
     p.cta_set_words = (uint32_t)value;
   else if (k == "stage_wait_polls" && value <= gary::kSpinLimit) p.stage_polls = (uint32_t)value;
   else if (k == "vertex_overhead") p.vertex_overhead = value;

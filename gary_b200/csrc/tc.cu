@@ -377,11 +377,11 @@ PlanParams resolve_params(PlanParams pp, uint64_t total_work) {
   // Measured on RMAT 18-24: the best warp tile holds about 1/32 of a resident
   // warp's share of the work (2^11 probes at RMAT-18 up to 2^15 at RMAT-22 and
   // above; larger tiles leave warps idle at the end, smaller ones pay the
-  // per-tile cost), and a third resident CTA per SM pays for its 40-register
-  // cap from about 2^31 probes (RMAT-22) on.
+  // per-tile cost), and three resident CTAs per SM (12 warps each, against two
+  // of 16) pay from about 2^31 probes (RMAT-22) on.
   if (pp.min_blocks != 2 && pp.min_blocks != 3) pp.min_blocks = total_work >= (1ull << 31) ? 3 : 2;
   if (!pp.warp_tile_cost) {
-    const uint64_t slots = (uint64_t)sm_count() * kTcWarps * pp.min_blocks;
+    const uint64_t slots = (uint64_t)sm_count() * tc_warps(pp.min_blocks) * pp.min_blocks;
     const uint64_t want = total_work / (slots * 32);
     uint64_t t = 1ull << 11;
     while (t < want && t < (1ull << 15)) t <<= 1;
@@ -425,7 +425,7 @@ int build_k3_plan(gary_graph *g, const PlanParams &pp_in, cudaStream_t s, gary_c
     GARY_CUDA(cudaGetLastError());
     const uint64_t total = thrust::reduce(pol, pcost.p, pcost.p + n, 0ull);
     // about 32 warp tiles per resident warp, in predicted cycles
-    const uint64_t slots = (uint64_t)sm_count() * pp.min_blocks * kTcWarps * 32;
+    const uint64_t slots = (uint64_t)sm_count() * pp.min_blocks * tc_warps(pp.min_blocks) * 32;
     tw = std::max<uint64_t>(total / std::max<uint64_t>(slots, 1), 4096);
     plan->learned = true;
   }
@@ -838,7 +838,7 @@ int k3_features(gary_graph *g, gary_count_plan *plan, float *d_x, uint8_t *d_leg
 template <int MINB>
 int launch_k3_impl(gary_graph *g, gary_count_plan *plan, unsigned long long *d_out, cudaStream_t s,
                    uint32_t shard, uint32_t nshards, VertexCtl ctl) {
-  constexpr int WARPS = kTcWarps;
+  constexpr int WARPS = tc_warps(MINB);
   auto kern = k_tc_mid<WARPS, MINB>;
   const size_t smem = (size_t)WARPS * kWarpTableSlots * 4;
   static bool attr_done[64] = {false};

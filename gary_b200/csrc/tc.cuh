@@ -8,7 +8,11 @@
 
 namespace gary {
 
-constexpr int kTcWarps = 16;               // warps per CTA of the counting kernel
+// Warps per CTA of the counting kernel at `min_blocks` CTAs per SM: 16 at 2;
+// 12 at 3, where 36 resident warps at 56 registers beat 48 warps held to 40
+// registers with spills (RMAT-24 ef32 122.7 -> 119.7 ms, RMAT-22 7.05 -> 6.77 ms).
+constexpr int tc_warps(int min_blocks) { return min_blocks >= 3 ? 12 : 16; }
+constexpr int kTcMaxWarps = 16;
 constexpr uint32_t kWarpTableSlots = 1024;  // per-warp shared set (4 KB)
 constexpr uint32_t kGroupTile = 0xFFFFFFFFu;
 constexpr uint32_t kMaxCountCtas = 1024;  // CTAs of a counting launch (SMs x resident CTAs)
