@@ -29,7 +29,8 @@ def _counts(ptr, idx, n):
         return g.count(K3), g.count(C4), g.count(K4)
 
 
-@pytest.mark.parametrize("n", [4, 5, 8, 13, 40])
+# 1100 and 1500: d+ up to 1499, past the 1024 whose bit rows fit shared memory (rows in HBM)
+@pytest.mark.parametrize("n", [4, 5, 8, 13, 40, 600, 1100, 1500])
 def test_complete_graphs(cuda, n):
     ptr, idx = _graph(n, list(itertools.combinations(range(n), 2)))
     assert _counts(ptr, idx, n) == (comb(n, 3), 3 * comb(n, 4), comb(n, 4))
