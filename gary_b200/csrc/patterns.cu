@@ -35,6 +35,7 @@
 // All counter traffic stays in shared memory; the lists stream from HBM.
 #include <thrust/binary_search.h>
 #include <thrust/copy.h>
+#include <thrust/count.h>
 #include <thrust/execution_policy.h>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
@@ -565,7 +566,8 @@ constexpr int kK4WarpCtaWarps = 8;
 constexpr int kK4MidThreads = 256, kK4MidLog = 10;
 constexpr uint32_t kK4MidRowWords = kK4MidMaxD * (kK4MidMaxD / 32);  // 8192
 constexpr int kK4BigThreads = 1024, kK4BigLog = 13;                 // d+ <= 4096
-constexpr uint32_t kK4BigRowWords = 32768;
+constexpr uint32_t kK4BigRowWords = 32768;  // rows in shared memory up to d+ = 1024
+constexpr uint32_t kK4PoolPerSm = 2;         // CTAs per SM of the HBM-row kernel
 static_assert(2 * (1u << kK4WarpLog) + kK4WarpMaxD * (kK4WarpMaxD / 32) <= kK4WarpWords,
               "warp region too small");
 static_assert((1u << kK4MidLog) >= 2 * kK4MidMaxD, "mid hash too small");
@@ -676,12 +678,14 @@ __device__ unsigned long long k4_vertex(const GraphView &g, uint32_t u, uint32_t
   return cnt;
 }
 
-// One listed vertex per CTA at a time, claimed through *counter.
+// One listed vertex per CTA at a time, claimed through *counter.  ROWW = 0:
+// every vertex keeps its rows in its CTA's HBM buffer, and the CTA holds only
+// the position hash in shared memory.
 template <int THREADS, int HLOG, uint32_t ROWW>
-__global__ void __launch_bounds__(THREADS)
-    k_k4_cta(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
-             uint32_t *__restrict__ pool, uint64_t pool_words, uint32_t *counter, unsigned *err,
-             unsigned long long *__restrict__ out) {
+__device__ __forceinline__ void k4_cta_body(GraphView g, const uint32_t *__restrict__ list, uint32_t lo,
+                                            uint32_t hi, uint32_t *__restrict__ pool, uint64_t pool_words,
+                                            uint32_t *counter, unsigned *err,
+                                            unsigned long long *__restrict__ out) {
   extern __shared__ __align__(16) uint32_t sm[];
   __shared__ uint32_t s_idx;
   uint32_t *keys = sm, *pos = sm + (1u << HLOG), *srows = sm + 2 * (1u << HLOG);
@@ -702,6 +706,22 @@ __global__ void __launch_bounds__(THREADS)
   }
   cnt = warp_sum_u64(cnt);
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
+template <int THREADS, int HLOG, uint32_t ROWW>
+__global__ void __launch_bounds__(THREADS)
+    k_k4_cta(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
+             uint32_t *__restrict__ pool, uint64_t pool_words, uint32_t *counter, unsigned *err,
+             unsigned long long *__restrict__ out) {
+  k4_cta_body<THREADS, HLOG, ROWW>(g, list, lo, hi, pool, pool_words, counter, err, out);
+}
+
+// Vertices whose rows live in HBM: two 1024-thread CTAs share an SM.
+__global__ void __launch_bounds__(kK4BigThreads, kK4PoolPerSm)
+    k_k4_pool(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
+              uint32_t *__restrict__ pool, uint64_t pool_words, uint32_t *counter, unsigned *err,
+              unsigned long long *__restrict__ out) {
+  k4_cta_body<kK4BigThreads, kK4BigLog, 0>(g, list, lo, hi, pool, pool_words, counter, err, out);
 }
 
 // Warp vertices: each warp in its own region of shared memory, 32 vertices per claim.
@@ -844,6 +864,10 @@ struct PreOf {
   const uint32_t *dplus;
   __host__ __device__ uint32_t operator()(uint32_t u) const { return srow[u].y - dplus[u]; }
 };
+struct RowsAbove {
+  uint32_t words;
+  __host__ __device__ bool operator()(uint32_t d) const { return (uint64_t)d * ((d + 31) / 32) > words; }
+};
 struct MaxU32 {
   __host__ __device__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
 };
@@ -890,11 +914,19 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
     GARY_CUDA(cudaMemcpyAsync(&dmax, key.p, 4, cudaMemcpyDeviceToHost, s));
     GARY_CUDA(cudaStreamSynchronize(s));
     plan->max_pre = dmax;
-    plan->win_ctas = (uint32_t)sm_count();
+    plan->n_pool = (uint32_t)thrust::count_if(pol, key.p, key.p + plan->n_big, RowsAbove{kK4BigRowWords});
+    plan->win_ctas = (uint32_t)sm_count() * kK4PoolPerSm;
     const uint64_t words = (uint64_t)dmax * ((dmax + 31) / 32);
-    if (words > kK4BigRowWords) {  // rows of the largest vertices live in HBM, one buffer per CTA
+    if (plan->n_pool) {  // rows of the largest vertices live in HBM, one buffer per CTA
       GARY_TRY(plan->cursors.alloc_persistent((uint64_t)plan->win_ctas * words));
       GARY_CUDA(cudaMemsetAsync(plan->cursors.p, 0, plan->cursors.bytes(), s));
+    }
+    if (plan->n_pool && plan->n_pool < plan->n_big) {
+      int least = 0, greatest = 0;
+      GARY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+      GARY_CUDA(cudaStreamCreateWithPriority(&plan->side.s, cudaStreamNonBlocking, greatest));
+      GARY_CUDA(cudaEventCreateWithFlags(&plan->side.fork, cudaEventDisableTiming));
+      GARY_CUDA(cudaEventCreateWithFlags(&plan->side.join, cudaEventDisableTiming));
     }
   }
   GARY_TRY(plan->sched.alloc_persistent(1));
@@ -906,10 +938,14 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
 int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaStream_t s,
               uint32_t shard, uint32_t nshards) {
   auto part = [&](uint32_t total, uint32_t k) { return (uint32_t)((uint64_t)total * k / nshards); };
-  const uint32_t b0 = part(plan->n_big, shard), b1 = part(plan->n_big, shard + 1);
+  const uint32_t np = plan->n_pool, ns = plan->n_big - plan->n_pool;
+  const uint32_t p0 = part(np, shard), p1 = part(np, shard + 1);
+  const uint32_t b0 = np + part(ns, shard), b1 = np + part(ns, shard + 1);
   const uint32_t m0 = part(plan->n_mid, shard), m1 = part(plan->n_mid, shard + 1);
   const uint32_t w0 = part(plan->n_light, shard), w1 = part(plan->n_light, shard + 1);
   auto big = k_k4_cta<kK4BigThreads, kK4BigLog, kK4BigRowWords>;
+  auto pool = k_k4_pool;
+  const size_t smem_pool = 2 * (1u << kK4BigLog) * 4;
   auto mid = k_k4_cta<kK4MidThreads, kK4MidLog, kK4MidRowWords>;
   const size_t smem_big = (2 * (1u << kK4BigLog) + kK4BigRowWords) * 4;
   const size_t smem_mid = (2 * (1u << kK4MidLog) + kK4MidRowWords) * 4;
@@ -918,11 +954,14 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   const int dev = device_ordinal();
   if (dev < 64 && !attr[dev]) {
     GARY_CUDA(cudaFuncSetAttribute(big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_big));
+    GARY_CUDA(cudaFuncSetAttribute(pool, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pool));
     GARY_CUDA(cudaFuncSetAttribute(mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mid));
     GARY_CUDA(cudaFuncSetAttribute(k_k4_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_warp));
     attr[dev] = true;
   }
-  int per_mid = 0, per_warp = 0;
+  int per_mid = 0, per_warp = 0, per_pool = 0;
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_pool, pool, kK4BigThreads, smem_pool));
+  per_pool = std::max(per_pool, 1);
   GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_mid, mid, kK4MidThreads, smem_mid));
   GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_warp, k_k4_warp, kK4WarpCtaWarps * 32,
                                                           smem_warp));
@@ -935,16 +974,28 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   GARY_CUDA(cudaMemsetAsync(d_out, 0, 8, s));
   GARY_CUDA(cudaEventRecord(g->ev0, s));
   const GraphView gv = g->view();
-  if (b1 > b0) {
-    // one CTA per SM; the pool holds one row buffer per CTA of the grid
-    const unsigned grid = std::min<unsigned>((unsigned)sm_count(), b1 - b0);
-    if (plan->cursors.p && grid > plan->win_ctas) {
-      set_error("4-clique row pool sized for %u CTAs, grid has %u", plan->win_ctas, grid);
+  // The HBM-row vertices are the largest; their kernel runs on the side
+  // stream (placed first), and the other kernels take the SMs it frees.
+  const bool fork = p1 > p0 && b1 > b0 && plan->side.s;
+  if (p1 > p0) {
+    // rows in HBM: the pool holds one row buffer per CTA of the grid
+    const unsigned grid = std::min<unsigned>({(unsigned)(sm_count() * per_pool), plan->win_ctas, p1 - p0});
+    if (!plan->cursors.p) {
+      set_error("4-clique row pool missing for %u vertices", p1 - p0);
       return GARY_ERR_INVALID;
     }
-    big<<<grid, kK4BigThreads, smem_big, s>>>(gv, plan->big.p, b0, b1, plan->cursors.p, pool_words,
-                                              &st->next_cta, &st->error, d_out);
+    cudaStream_t ps = s;
+    if (fork) {
+      GARY_CUDA(cudaEventRecord(plan->side.fork, s));
+      GARY_CUDA(cudaStreamWaitEvent(plan->side.s, plan->side.fork, 0));
+      ps = plan->side.s;
+    }
+    pool<<<grid, kK4BigThreads, smem_pool, ps>>>(gv, plan->big.p, p0, p1, plan->cursors.p, pool_words,
+                                                 &st->next_cta, &st->error, d_out);
   }
+  if (b1 > b0)  // rows in shared memory, one CTA per SM
+    big<<<std::min<unsigned>((unsigned)sm_count(), b1 - b0), kK4BigThreads, smem_big, s>>>(
+        gv, plan->big.p, b0, b1, nullptr, 0, &st->next_big, &st->error, d_out);
   if (m1 > m0)
     mid<<<std::min<unsigned>((unsigned)(sm_count() * per_mid), m1 - m0), kK4MidThreads, smem_mid, s>>>(
         gv, plan->mid.p, m0, m1, nullptr, 0, &st->next_aux, &st->error, d_out);
@@ -952,10 +1003,14 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
     k_k4_warp<<<(unsigned)(sm_count() * per_warp), kK4WarpCtaWarps * 32, smem_warp, s>>>(
         gv, plan->light.p, w0, w1, &st->next_warp, &st->error, d_out);
   GARY_CUDA(cudaGetLastError());
+  if (fork) {
+    GARY_CUDA(cudaEventRecord(plan->side.join, plan->side.s));
+    GARY_CUDA(cudaStreamWaitEvent(s, plan->side.join, 0));
+  }
   GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
-  g->last.tiles = (b1 - b0) + (m1 - m0) + (w1 - w0);
-  g->last.cta_tiles = (b1 - b0) + (m1 - m0);
+  g->last.tiles = (p1 - p0) + (b1 - b0) + (m1 - m0) + (w1 - w0);
+  g->last.cta_tiles = (p1 - p0) + (b1 - b0) + (m1 - m0);
   g->last_timed = true;
   g->last_sched = st;
   g->last_span = nullptr;

@@ -10,16 +10,33 @@ namespace gary {
 // Largest d+(u) the 4-clique kernel supports (a CTA-wide table of 8192 slots).
 constexpr uint32_t kK4MaxOutDegree = 4096;
 
+// A second stream forked from and joined back into the caller's, for two
+// kernels of one count that may run side by side; created with the device's
+// highest priority, so that its CTAs are placed first.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  SideStream() = default;
+  SideStream(const SideStream &) = delete;
+  SideStream &operator=(const SideStream &) = delete;
+  ~SideStream() {
+    if (join) cudaEventDestroy(join);
+    if (fork) cudaEventDestroy(fork);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
 struct PatternPlan {
   // K4: CTA tiles then warp tiles.  C4: window tiles of heavy vertices, as
   // {v0 = u, v1 = |N(u) below u|, j0 = first window, j1 = end window}.
   DevBuf<Tile> tiles;
   DevBuf<uint32_t> light;    // light vertices (K4 groups index it; C4 warps walk it)
   DevBuf<uint32_t> mid;      // C4: medium vertices, one CTA hash map each; K4: mid vertices
-  DevBuf<uint32_t> big;      // K4: vertices with d+ > 512, largest first
+  DevBuf<uint32_t> big;      // K4: vertices with d+ > 512, largest first (the n_pool with rows in HBM first)
   DevBuf<uint32_t> cursors;  // C4: per window-kernel CTA, 6 x max_pre words of list state; K4: row pool
   DevBuf<SchedState> sched;
-  uint32_t n_cta = 0, n_warp = 0, n_light = 0, n_mid = 0, n_big = 0, max_pre = 0, win_ctas = 0;
+  SideStream side;           // K4: the HBM-row kernel beside the shared-row one
+  uint32_t n_cta = 0, n_warp = 0, n_light = 0, n_mid = 0, n_big = 0, n_pool = 0, max_pre = 0, win_ctas = 0;
 };
 
 int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out);

@@ -91,6 +91,7 @@ struct SchedState {
   uint32_t error;     // kLaunchErr* bits
   uint32_t next_aux;  // a third queue (the 4-cycle kernel's medium vertices)
   uint32_t cta_path[4];  // triangle CTA tiles by the set that held N+(v) (kPath*)
+  uint32_t next_big;     // a fourth queue (4-clique vertices whose rows fit shared memory)
 };
 
 // Sets a triangle CTA tile can hold N+(v) in, cheapest first.
