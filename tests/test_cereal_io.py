@@ -69,6 +69,22 @@ def test_read_packed_coo(tmp_path):
         gb.read_bin_csr(f)
 
 
+def test_committed_fixture():
+    """The committed fixture (tests/golden/make_cereal_fixture.py, written from
+    cereal's binary rules with the standard library only) reads back as the
+    graph it was made from, and writing that graph gives the same bytes."""
+    import json
+    from pathlib import Path
+
+    g = Path(__file__).parent / "golden"
+    want = json.loads((g / "cereal_csr_dag.json").read_text())
+    f = g / "cereal_csr_dag.bin"
+    assert gb.bin_info(f) == (gb.GARY_BIN_CSR, want["n"], len(want["indices"]))
+    p, i = gb.read_bin_csr(f)
+    assert p.tolist() == want["indptr"] and i.tolist() == want["indices"]
+    assert _csr_bytes(p, i) == f.read_bytes()
+
+
 def test_empty_graph(tmp_path):
     f = tmp_path / "empty.bin"
     f.write_bytes(_csr_bytes(np.zeros(4, np.int64), np.zeros(0, np.int32)))
