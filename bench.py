@@ -192,7 +192,7 @@ def workload_config(args, world: int) -> dict:
 # profiles/ applies to the build whose sources hash to its "kernel_src".
 KERNEL_SOURCES = ("tc.cu", "tc.cuh", "warp_ops.cuh", "bulk.cuh", "internal.cuh", "graph.cuh")
 # the 4-cycle and 4-clique count kernels
-PATTERN_SOURCES = ("patterns.cu", "patterns.cuh", "warp_ops.cuh", "internal.cuh", "graph.cuh")
+PATTERN_SOURCES = ("patterns.cu", "patterns.cuh", "pattern_rules.cuh", "warp_ops.cuh", "internal.cuh", "graph.cuh")
 
 
 def kernel_source_hash(sources=KERNEL_SOURCES) -> str:

@@ -57,7 +57,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kPWarps = 8;
-constexpr uint32_t kPSlots = 1024;  // per-warp hash slots
+constexpr uint32_t kPSlots = kC4WarpSlots;  // per-warp hash slots
+static_assert(kPSlots == 1u << 10, "warp map lookups hash to 10 bits");
 
 inline unsigned grid_for(uint64_t items) {
   uint64_t b = (items + kThreads - 1) / kThreads;
@@ -191,10 +192,11 @@ __global__ void __launch_bounds__(kPWarps * 32)
 // A count c(u,w) never exceeds the vertex's wedge count (each v adds at most
 // one to it), at most kMidWedges here, so counts are 16 bits, two to a word:
 // keys 64 KiB + counts 32 KiB, and two CTAs share an SM.
-constexpr uint32_t kMidSlots = 16384;
+constexpr uint32_t kMidSlots = kC4MidSlots;
 constexpr int kMidLog = 14;
+static_assert((1u << kMidLog) == kMidSlots, "medium map size");
 constexpr int kMidThreads = 512;
-constexpr uint64_t kMidWedges = kMidSlots / 2;  // wedges (>= distinct w) a medium vertex may have
+constexpr uint64_t kMidWedges = kC4MidWedges;  // wedges (>= distinct w) a medium vertex may have
 constexpr uint32_t kMidWords = kMidSlots + kMidSlots / 2;
 static_assert(kMidWedges < 65536, "16-bit medium counts");
 
@@ -269,7 +271,6 @@ __global__ void __launch_bounds__(kMidThreads, 2)
 // window is counted in two halves of kWinWords 32-bit counters.
 constexpr uint32_t kWinIds = 32 * 1024;
 constexpr uint32_t kWinWords = 16 * 1024;
-constexpr uint32_t kWin16MaxPre = 0xFFFFu;
 constexpr int kWinThreads = 512;
 constexpr int kWinWarps = kWinThreads / 32;
 
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(kWinThreads, 3)
     if (t >= t_hi) break;
     const Tile tl = tiles[t];
     const uint32_t u = tl.v0, pre = tl.v1;
-    const bool wide = pre > kWin16MaxPre;
+    const bool wide = c4_wide_counters(pre);
     const uint32_t ws = wide ? kWinIds / 2 : kWinIds;  // ids per pass
     const uint32_t *au = s.adj + (uint64_t)s.row[u].x * 4;
     const uint64_t end64 = (uint64_t)tl.j1 * kWinIds, begin64 = (uint64_t)tl.j0 * kWinIds;
@@ -558,19 +559,13 @@ __global__ void __launch_bounds__(kWinThreads, 3)
 //     shared memory, several CTAs per SM (one waits at a barrier, others run);
 //   big vertices (d+ > 512): a 1024-thread CTA each, rows in shared memory up
 //     to d+ = 1024 and in a per-CTA HBM buffer beyond.
-constexpr uint32_t kK4WarpMaxD = 128;         // warp vertices: rows of at most 4 words
-constexpr uint32_t kK4MidMaxD = 512;          // mid vertices: rows of at most 16 words
-constexpr int kK4WarpLog = 8;                 // warp position hash: 256 slots
+// (class bounds, table sizes and row words: pattern_rules.cuh)
 constexpr uint32_t kK4WarpWords = 1024;       // shared words per warp: 32 KiB per CTA, up to 7 CTAs per SM
 constexpr int kK4WarpCtaWarps = 8;
-constexpr int kK4MidThreads = 256, kK4MidLog = 10;
-constexpr uint32_t kK4MidRowWords = kK4MidMaxD * (kK4MidMaxD / 32);  // 8192
-constexpr int kK4BigThreads = 1024, kK4BigLog = 13;                 // d+ <= 4096
-constexpr uint32_t kK4BigRowWords = 32768;  // rows in shared memory up to d+ = 1024
+constexpr int kK4MidThreads = 256;
+constexpr int kK4BigThreads = 1024;
 constexpr uint32_t kK4PoolPerSm = 2;         // CTAs per SM of the HBM-row kernel
-static_assert(2 * (1u << kK4WarpLog) + kK4WarpMaxD * (kK4WarpMaxD / 32) <= kK4WarpWords,
-              "warp region too small");
-static_assert((1u << kK4MidLog) >= 2 * kK4MidMaxD, "mid hash too small");
+static_assert(2 * (1u << kK4WarpLog) + kK4WarpRowWords <= kK4WarpWords, "warp region too small");
 
 // Position hash of N+(u) (ids are distinct).  k4_vertex inserts at most
 // half as many ids as the table has slots, so every lookup ends at a free
@@ -768,7 +763,10 @@ __global__ void k_c4_classify(const uint2 *__restrict__ srow, const uint32_t *__
     const uint32_t pre = r.y - dplus[u];
     uint64_t w = 0;
     for (uint32_t k = 0; k < pre && w <= warp_cap; ++k) w += srow[sadj[(uint64_t)r.x * 4 + k]].y;
-    cls[u] = pre == 0 ? kClassNone : (w <= warp_cap ? kClassLight : kClassCta);
+    // w: the wedge bound, its sum stopped once past the light limit; the
+    // exact counts that split the others come later
+    const C4Class c = c4_class(pre, w, ~0ull);
+    cls[u] = c == kC4None ? kClassNone : (c == kC4Light ? kClassLight : kClassCta);
   }
 }
 
@@ -842,10 +840,13 @@ __global__ void k_c4_fill_tiles(const uint2 *__restrict__ srow, const uint32_t *
   }
 }
 
-struct DegIn {
+struct K4WorkerIn {
   const uint32_t *d;
-  uint32_t lo, hi;
-  __host__ __device__ bool operator()(uint32_t u) const { return d[u] >= lo && d[u] <= hi; }
+  K4Worker lo, hi;
+  __host__ __device__ bool operator()(uint32_t u) const {
+    const K4Worker w = k4_worker(d[u]);
+    return w >= lo && w <= hi;
+  }
 };
 struct DegOf {
   const uint32_t *d;
@@ -864,9 +865,8 @@ struct PreOf {
   const uint32_t *dplus;
   __host__ __device__ uint32_t operator()(uint32_t u) const { return srow[u].y - dplus[u]; }
 };
-struct RowsAbove {
-  uint32_t words;
-  __host__ __device__ bool operator()(uint32_t d) const { return (uint64_t)d * ((d + 31) / 32) > words; }
+struct K4PoolDegree {
+  __host__ __device__ bool operator()(uint32_t d) const { return k4_worker(d) == kK4Pool; }
 };
 struct MaxU32 {
   __host__ __device__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
@@ -896,15 +896,15 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
   GARY_TRY(plan->light.alloc_persistent(std::max<uint32_t>(n, 1)));
   plan->n_light = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
                                              thrust::counting_iterator<uint32_t>(n), plan->light.p,
-                                             DegIn{dp, 3, kK4WarpMaxD}) - plan->light.p);
+                                             K4WorkerIn{dp, kK4Warp, kK4Warp}) - plan->light.p);
   GARY_TRY(plan->mid.alloc_persistent(std::max<uint32_t>(n, 1)));
   plan->n_mid = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
                                            thrust::counting_iterator<uint32_t>(n), plan->mid.p,
-                                           DegIn{dp, kK4WarpMaxD + 1, kK4MidMaxD}) - plan->mid.p);
+                                           K4WorkerIn{dp, kK4Mid, kK4Mid}) - plan->mid.p);
   GARY_TRY(plan->big.alloc_persistent(std::max<uint32_t>(n, 1)));
   plan->n_big = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),
                                            thrust::counting_iterator<uint32_t>(n), plan->big.p,
-                                           DegIn{dp, kK4MidMaxD + 1, 0xFFFFFFFFu}) - plan->big.p);
+                                           K4WorkerIn{dp, kK4Big, kK4Pool}) - plan->big.p);
   if (plan->n_big) {
     DevBuf<uint32_t> key;
     GARY_TRY(key.alloc(plan->n_big, s));
@@ -914,7 +914,7 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
     GARY_CUDA(cudaMemcpyAsync(&dmax, key.p, 4, cudaMemcpyDeviceToHost, s));
     GARY_CUDA(cudaStreamSynchronize(s));
     plan->max_pre = dmax;
-    plan->n_pool = (uint32_t)thrust::count_if(pol, key.p, key.p + plan->n_big, RowsAbove{kK4BigRowWords});
+    plan->n_pool = (uint32_t)thrust::count_if(pol, key.p, key.p + plan->n_big, K4PoolDegree{});
     plan->win_ctas = (uint32_t)sm_count() * kK4PoolPerSm;
     const uint64_t words = (uint64_t)dmax * ((dmax + 31) / 32);
     if (plan->n_pool) {  // rows of the largest vertices live in HBM, one buffer per CTA
@@ -1026,7 +1026,7 @@ int build_c4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
   DevBuf<uint8_t> cls;
   GARY_TRY(cls.alloc(n, s));
   k_c4_classify<<<grid_for(n), kThreads, 0, s>>>(g->sym.row.p, g->sym.adj.p, g->dag.outdeg.p, n,
-                                                 kPSlots / 2, cls.p);
+                                                 (uint32_t)kC4LightWedges, cls.p);
   GARY_CUDA(cudaGetLastError());
   GARY_TRY(plan->light.alloc_persistent(std::max<uint32_t>(n, 1)));
   plan->n_light = (uint32_t)(thrust::copy_if(pol, thrust::counting_iterator<uint32_t>(0),

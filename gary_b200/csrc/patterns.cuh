@@ -3,12 +3,10 @@
 #include <cstdint>
 
 #include "graph.cuh"
+#include "pattern_rules.cuh"
 #include "tc.cuh"
 
 namespace gary {
-
-// Largest d+(u) the 4-clique kernel supports (a CTA-wide table of 8192 slots).
-constexpr uint32_t kK4MaxOutDegree = 4096;
 
 // A second stream forked from and joined back into the caller's, for two
 // kernels of one count that may run side by side; created with the device's
