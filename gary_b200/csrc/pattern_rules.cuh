@@ -42,12 +42,14 @@ constexpr uint32_t kK4WarpMaxD = 128;  // one warp per vertex up to here
 constexpr uint32_t kK4MidMaxD = 512;   // a 256-thread CTA up to here, a 1024-thread CTA beyond
 constexpr int kK4WarpLog = 8;          // position hash slots (log2) of each worker
 constexpr int kK4MidLog = 10;
-constexpr int kK4BigLog = 13;
+constexpr int kK4BigLog = 11;          // shared-row vertices: d+ <= 877
+constexpr int kK4PoolLog = 13;         // HBM-row vertices: d+ <= 4096
 // Shared words for bit rows: a warp's region, the 256-thread CTA's, the
-// 1024-thread CTA's.  Past the last, rows live in an HBM buffer per CTA.
+// 1024-thread CTA's (96 KiB, so that two CTAs share an SM).  Past the last,
+// rows live in an HBM buffer per CTA.
 constexpr uint32_t kK4WarpRowWords = kK4WarpMaxD * (kK4WarpMaxD / 32);  // 512
 constexpr uint32_t kK4MidRowWords = kK4MidMaxD * (kK4MidMaxD / 32);     // 8192
-constexpr uint32_t kK4BigRowWords = 32768;
+constexpr uint32_t kK4BigRowWords = 24576;
 
 enum K4Worker : uint8_t { kK4None = 0, kK4Warp = 1, kK4Mid = 2, kK4Big = 3, kK4Pool = 4 };
 
@@ -64,7 +66,7 @@ __host__ __device__ constexpr K4Worker k4_worker(uint32_t d) {
 }
 
 __host__ __device__ constexpr int k4_table_log(K4Worker w) {
-  return w == kK4Warp ? kK4WarpLog : w == kK4Mid ? kK4MidLog : kK4BigLog;
+  return w == kK4Warp ? kK4WarpLog : w == kK4Mid ? kK4MidLog : w == kK4Big ? kK4BigLog : kK4PoolLog;
 }
 
 // Shared row words of a worker (0: rows in its HBM buffer).

@@ -557,8 +557,10 @@ __global__ void __launch_bounds__(kWinThreads, 3)
 //   warp vertices (3 <= d+ <= 128): one warp each, 8-warp CTAs, several per SM;
 //   mid vertices (128 < d+ <= 512): a 256-thread CTA each, rows in 32 KiB of
 //     shared memory, several CTAs per SM (one waits at a barrier, others run);
-//   big vertices (d+ > 512): a 1024-thread CTA each, rows in shared memory up
-//     to d+ = 1024 and in a per-CTA HBM buffer beyond.
+//   big vertices (d+ > 512): a 1024-thread CTA each, two per SM: rows in 96
+//     KiB of shared memory up to d+ = 877; beyond, rows in a per-CTA HBM buffer
+//     and only the position hash in shared memory (k_k4_pool, run first: its
+//     vertices are the largest).
 // (class bounds, table sizes and row words: pattern_rules.cuh)
 constexpr uint32_t kK4WarpWords = 1024;       // shared words per warp: 32 KiB per CTA, up to 7 CTAs per SM
 constexpr int kK4WarpCtaWarps = 8;
@@ -716,7 +718,7 @@ __global__ void __launch_bounds__(kK4BigThreads, kK4PoolPerSm)
     k_k4_pool(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
               uint32_t *__restrict__ pool, uint64_t pool_words, uint32_t *counter, unsigned *err,
               unsigned long long *__restrict__ out) {
-  k4_cta_body<kK4BigThreads, kK4BigLog, 0>(g, list, lo, hi, pool, pool_words, counter, err, out);
+  k4_cta_body<kK4BigThreads, kK4PoolLog, 0>(g, list, lo, hi, pool, pool_words, counter, err, out);
 }
 
 // Warp vertices: each warp in its own region of shared memory, 32 vertices per claim.
@@ -921,13 +923,6 @@ int build_k4_plan(gary_graph *g, cudaStream_t s, PatternPlan **out) {
       GARY_TRY(plan->cursors.alloc_persistent((uint64_t)plan->win_ctas * words));
       GARY_CUDA(cudaMemsetAsync(plan->cursors.p, 0, plan->cursors.bytes(), s));
     }
-    if (plan->n_pool && plan->n_pool < plan->n_big) {
-      int least = 0, greatest = 0;
-      GARY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-      GARY_CUDA(cudaStreamCreateWithPriority(&plan->side.s, cudaStreamNonBlocking, greatest));
-      GARY_CUDA(cudaEventCreateWithFlags(&plan->side.fork, cudaEventDisableTiming));
-      GARY_CUDA(cudaEventCreateWithFlags(&plan->side.join, cudaEventDisableTiming));
-    }
   }
   GARY_TRY(plan->sched.alloc_persistent(1));
   GARY_CUDA(cudaStreamSynchronize(s));
@@ -945,7 +940,7 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   const uint32_t w0 = part(plan->n_light, shard), w1 = part(plan->n_light, shard + 1);
   auto big = k_k4_cta<kK4BigThreads, kK4BigLog, kK4BigRowWords>;
   auto pool = k_k4_pool;
-  const size_t smem_pool = 2 * (1u << kK4BigLog) * 4;
+  const size_t smem_pool = 2 * (1u << kK4PoolLog) * 4;
   auto mid = k_k4_cta<kK4MidThreads, kK4MidLog, kK4MidRowWords>;
   const size_t smem_big = (2 * (1u << kK4BigLog) + kK4BigRowWords) * 4;
   const size_t smem_mid = (2 * (1u << kK4MidLog) + kK4MidRowWords) * 4;
@@ -959,7 +954,9 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
     GARY_CUDA(cudaFuncSetAttribute(k_k4_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_warp));
     attr[dev] = true;
   }
-  int per_mid = 0, per_warp = 0, per_pool = 0;
+  int per_mid = 0, per_warp = 0, per_pool = 0, per_big = 0;
+  GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_big, big, kK4BigThreads, smem_big));
+  per_big = std::max(per_big, 1);
   GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_pool, pool, kK4BigThreads, smem_pool));
   per_pool = std::max(per_pool, 1);
   GARY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_mid, mid, kK4MidThreads, smem_mid));
@@ -974,9 +971,7 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
   GARY_CUDA(cudaMemsetAsync(d_out, 0, 8, s));
   GARY_CUDA(cudaEventRecord(g->ev0, s));
   const GraphView gv = g->view();
-  // The HBM-row vertices are the largest; their kernel runs on the side
-  // stream (placed first), and the other kernels take the SMs it frees.
-  const bool fork = p1 > p0 && b1 > b0 && plan->side.s;
+  // The HBM-row vertices are the largest: their kernel runs first.
   if (p1 > p0) {
     // rows in HBM: the pool holds one row buffer per CTA of the grid
     const unsigned grid = std::min<unsigned>({(unsigned)(sm_count() * per_pool), plan->win_ctas, p1 - p0});
@@ -984,17 +979,11 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
       set_error("4-clique row pool missing for %u vertices", p1 - p0);
       return GARY_ERR_INVALID;
     }
-    cudaStream_t ps = s;
-    if (fork) {
-      GARY_CUDA(cudaEventRecord(plan->side.fork, s));
-      GARY_CUDA(cudaStreamWaitEvent(plan->side.s, plan->side.fork, 0));
-      ps = plan->side.s;
-    }
-    pool<<<grid, kK4BigThreads, smem_pool, ps>>>(gv, plan->big.p, p0, p1, plan->cursors.p, pool_words,
-                                                 &st->next_cta, &st->error, d_out);
+    pool<<<grid, kK4BigThreads, smem_pool, s>>>(gv, plan->big.p, p0, p1, plan->cursors.p, pool_words,
+                                                &st->next_cta, &st->error, d_out);
   }
-  if (b1 > b0)  // rows in shared memory, one CTA per SM
-    big<<<std::min<unsigned>((unsigned)sm_count(), b1 - b0), kK4BigThreads, smem_big, s>>>(
+  if (b1 > b0)  // rows in shared memory, two CTAs per SM
+    big<<<std::min<unsigned>((unsigned)(sm_count() * per_big), b1 - b0), kK4BigThreads, smem_big, s>>>(
         gv, plan->big.p, b0, b1, nullptr, 0, &st->next_big, &st->error, d_out);
   if (m1 > m0)
     mid<<<std::min<unsigned>((unsigned)(sm_count() * per_mid), m1 - m0), kK4MidThreads, smem_mid, s>>>(
@@ -1003,10 +992,6 @@ int launch_k4(gary_graph *g, PatternPlan *plan, unsigned long long *d_out, cudaS
     k_k4_warp<<<(unsigned)(sm_count() * per_warp), kK4WarpCtaWarps * 32, smem_warp, s>>>(
         gv, plan->light.p, w0, w1, &st->next_warp, &st->error, d_out);
   GARY_CUDA(cudaGetLastError());
-  if (fork) {
-    GARY_CUDA(cudaEventRecord(plan->side.join, plan->side.s));
-    GARY_CUDA(cudaStreamWaitEvent(s, plan->side.join, 0));
-  }
   GARY_CUDA(cudaEventRecord(g->ev1, s));
   g->last = gary_count_stats{};
   g->last.tiles = (p1 - p0) + (b1 - b0) + (m1 - m0) + (w1 - w0);

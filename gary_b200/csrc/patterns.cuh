@@ -8,22 +8,6 @@
 
 namespace gary {
 
-// A second stream forked from and joined back into the caller's, for two
-// kernels of one count that may run side by side; created with the device's
-// highest priority, so that its CTAs are placed first.
-struct SideStream {
-  cudaStream_t s = nullptr;
-  cudaEvent_t fork = nullptr, join = nullptr;
-  SideStream() = default;
-  SideStream(const SideStream &) = delete;
-  SideStream &operator=(const SideStream &) = delete;
-  ~SideStream() {
-    if (join) cudaEventDestroy(join);
-    if (fork) cudaEventDestroy(fork);
-    if (s) cudaStreamDestroy(s);
-  }
-};
-
 struct PatternPlan {
   // K4: CTA tiles then warp tiles.  C4: window tiles of heavy vertices, as
   // {v0 = u, v1 = |N(u) below u|, j0 = first window, j1 = end window}.
@@ -33,7 +17,6 @@ struct PatternPlan {
   DevBuf<uint32_t> big;      // K4: vertices with d+ > 512, largest first (the n_pool with rows in HBM first)
   DevBuf<uint32_t> cursors;  // C4: per window-kernel CTA, 6 x max_pre words of list state; K4: row pool
   DevBuf<SchedState> sched;
-  SideStream side;           // K4: the HBM-row kernel beside the shared-row one
   uint32_t n_cta = 0, n_warp = 0, n_light = 0, n_mid = 0, n_big = 0, n_pool = 0, max_pre = 0, win_ctas = 0;
 };
 

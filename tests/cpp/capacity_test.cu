@@ -46,12 +46,14 @@ static void k4_rules() {
   }
   CHECK(k4_worker(kK4WarpMaxD) == kK4Warp && k4_worker(kK4WarpMaxD + 1) == kK4Mid, "warp/mid boundary");
   CHECK(k4_worker(kK4MidMaxD) == kK4Mid && k4_worker(kK4MidMaxD + 1) == kK4Big, "mid/big boundary");
-  CHECK(k4_worker(1024) == kK4Big && k4_worker(1025) == kK4Pool, "shared/HBM row boundary at d+ = 1024");
+  CHECK(k4_worker(877) == kK4Big && k4_worker(878) == kK4Pool, "shared/HBM row boundary at d+ = 877");
   // the HBM buffer of a CTA is sized for the graph's largest d+; every pool
   // vertex's rows must fit it
-  for (uint32_t dmax : {1025u, 1500u, 3124u, kK4MaxOutDegree}) {
+  uint32_t first_pool = kK4MidMaxD;
+  while (k4_worker(first_pool) != kK4Pool) ++first_pool;
+  for (uint32_t dmax : {first_pool, 1500u, 3124u, kK4MaxOutDegree}) {
     const uint64_t pool = (uint64_t)dmax * k4_row_words(dmax);
-    for (uint32_t d = 1025; d <= dmax; ++d)
+    for (uint32_t d = first_pool; d <= dmax; ++d)
       CHECK((uint64_t)d * k4_row_words(d) <= pool, "d=%u rows exceed the buffer sized for %u", d, dmax);
   }
 }
