@@ -39,7 +39,7 @@ __host__ __device__ constexpr bool c4_wide_counters(uint32_t pre) { return pre >
 // Largest d+(u) the 4-clique kernels take (the API refuses larger graphs).
 constexpr uint32_t kK4MaxOutDegree = 4096;
 constexpr uint32_t kK4WarpMaxD = 128;  // one warp per vertex up to here
-constexpr uint32_t kK4MidMaxD = 512;   // a 256-thread CTA up to here, a 1024-thread CTA beyond
+constexpr uint32_t kK4MidMaxD = 362;   // a 256-thread CTA up to here, a 1024-thread CTA beyond
 constexpr int kK4WarpLog = 8;          // position hash slots (log2) of each worker
 constexpr int kK4MidLog = 10;
 constexpr int kK4BigLog = 11;          // shared-row vertices: d+ <= 877
@@ -47,8 +47,8 @@ constexpr int kK4PoolLog = 13;         // HBM-row vertices: d+ <= 4096
 // Shared words for bit rows: a warp's region, the 256-thread CTA's, the
 // 1024-thread CTA's (96 KiB, so that two CTAs share an SM).  Past the last,
 // rows live in an HBM buffer per CTA.
-constexpr uint32_t kK4WarpRowWords = kK4WarpMaxD * (kK4WarpMaxD / 32);  // 512
-constexpr uint32_t kK4MidRowWords = kK4MidMaxD * (kK4MidMaxD / 32);     // 8192
+constexpr uint32_t kK4WarpRowWords = kK4WarpMaxD * ((kK4WarpMaxD + 31) / 32);  // 512
+constexpr uint32_t kK4MidRowWords = kK4MidMaxD * ((kK4MidMaxD + 31) / 32);
 constexpr uint32_t kK4BigRowWords = 24576;
 
 enum K4Worker : uint8_t { kK4None = 0, kK4Warp = 1, kK4Mid = 2, kK4Big = 3, kK4Pool = 4 };

@@ -555,9 +555,9 @@ __global__ void __launch_bounds__(kWinThreads, 3)
 // ---- K4: bit rows of the subgraph induced by N+(u) -------------------------
 // Three sizes of worker, so that no worker waits at barriers it does not need:
 //   warp vertices (3 <= d+ <= 128): one warp each, 8-warp CTAs, several per SM;
-//   mid vertices (128 < d+ <= 512): a 256-thread CTA each, rows in 32 KiB of
-//     shared memory, several CTAs per SM (one waits at a barrier, others run);
-//   big vertices (d+ > 512): a 1024-thread CTA each, two per SM: rows in 96
+//   mid vertices (128 < d+ <= 362): a 256-thread CTA each, rows in 17 KiB of
+//     shared memory, eight CTAs per SM (one waits at a barrier, others run);
+//   big vertices (d+ > 362): a 1024-thread CTA each, two per SM: rows in 96
 //     KiB of shared memory up to d+ = 877; beyond, rows in a per-CTA HBM buffer
 //     and only the position hash in shared memory (k_k4_pool, run first: its
 //     vertices are the largest).
