@@ -721,7 +721,8 @@ __global__ void __launch_bounds__(kK4BigThreads, kK4PoolPerSm)
   k4_cta_body<kK4BigThreads, kK4PoolLog, 0>(g, list, lo, hi, pool, pool_words, counter, err, out);
 }
 
-// Warp vertices: each warp in its own region of shared memory, 32 vertices per claim.
+// Warp vertices: each warp in its own region of shared memory, one vertex per
+// claim (32 per claim left a tail of costly vertices: RMAT-22 129.1 -> 119.6 ms).
 __global__ void __launch_bounds__(kK4WarpCtaWarps * 32)
     k_k4_warp(GraphView g, const uint32_t *__restrict__ list, uint32_t lo, uint32_t hi,
               uint32_t *counter, unsigned *err, unsigned long long *__restrict__ out) {
@@ -735,15 +736,10 @@ __global__ void __launch_bounds__(kK4WarpCtaWarps * 32)
   unsigned long long cnt = 0;
   while (true) {
     uint32_t c = 0;
-    if (lane == 0) c = atomicAdd(counter, 32u);
+    if (lane == 0) c = atomicAdd(counter, 1u);
     c = __shfl_sync(kFull, c, 0);
-    const uint32_t i0 = lo + c;
-    if (i0 >= hi) break;
-    const uint32_t nb = min(32u, hi - i0);
-    const uint32_t myu = lane < nb ? list[i0 + lane] : 0u;
-    for (uint32_t q = 0; q < nb; ++q)
-      cnt += k4_vertex(g, __shfl_sync(kFull, myu, q), keys, pos, kK4WarpLog, rows, lane, 32,
-                       [] { __syncwarp(); }, err);
+    if (lo + c >= hi) break;
+    cnt += k4_vertex(g, list[lo + c], keys, pos, kK4WarpLog, rows, lane, 32, [] { __syncwarp(); }, err);
   }
   cnt = warp_sum_u64(cnt);
   if (lane == 0 && cnt) atomicAdd(out, cnt);
