@@ -7,7 +7,7 @@
 
 Training data is logged by the instrumented plain kernel itself: for every
 middle vertex of the triangle kernel, clock64 cycles with each intersection
-variant forced in turn (hash, search, merge, bitmap), next to the vertex's
+variant forced in turn (hash, search, regs: at most 8 ids in registers, bitmap), next to the vertex's
 six features.  A sample carries targets only for the variants that are legal
 for it.  The network predicts log2 cycles per variant; GARY_SCHED_LEARNED
 picks the cheapest legal variant per vertex and weights tiles by it.
@@ -25,7 +25,7 @@ import numpy as np
 from ._lib import GARY_PATTERN_TRIANGLE, GARY_SCHED_LEARNED, GARY_SCHED_PLAIN, check, load
 
 N_IN, N_OUT = 6, 4
-VARIANTS = ("hash", "search", "merge", "bitmap")
+VARIANTS = ("hash", "search", "regs", "bitmap")
 DEFAULT_MODEL = Path(__file__).resolve().parent / "data" / "cost_model.gmlp"
 
 

@@ -676,8 +676,8 @@ struct SmemSearchSet {
   }
 };
 
-// Up to 8 ids held in registers, compared directly (variant MERGE: a merge
-// against a list short enough to keep whole in every lane).
+// Up to 8 ids held in registers in every lane, each probe compared against
+// all of them (variant REGS).
 struct RegSet8 {
   uint32_t r[8];
   __device__ __forceinline__ uint32_t contains(uint32_t x) const {

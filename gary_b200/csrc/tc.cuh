@@ -20,7 +20,7 @@ constexpr uint32_t kMaxCountCtas = 1024;  // CTAs of a counting launch (SMs x re
 enum : uint8_t { kClassNone = 0, kClassLight = 1, kClassSplit = 2, kClassCta = 3 };
 
 // Intersection variants a tile can run (the cost model's output order).
-enum : uint32_t { kVarHash = 0, kVarSearch = 1, kVarMerge = 2, kVarBitmap = 3 };
+enum : uint32_t { kVarHash = 0, kVarSearch = 1, kVarRegs = 2, kVarBitmap = 3 };
 
 // Can a warp run middle vertex v (d = d+(v), span = id span of N+(v)) with
 // variant `var`?  Sizes follow the warp's kWarpTableSlots shared words.
@@ -28,7 +28,7 @@ __host__ __device__ __forceinline__ bool variant_legal(uint32_t var, uint32_t d,
   switch (var) {
     case kVarHash: return d <= kWarpTableSlots / 2;
     case kVarSearch: return d <= kWarpTableSlots;
-    case kVarMerge: return d <= 8;
+    case kVarRegs: return d <= 8;
     case kVarBitmap: return span <= (kWarpTableSlots - 1) * 32u - 1u;
     default: return false;
   }

@@ -325,7 +325,7 @@ int gary_gen_pairs_values(uint64_t seed, uint64_t first, uint64_t npairs, uint32
 /* ---- learned scheduling: the cost model ---------------------------------
  * A 6 -> 64 -> 64 -> 4 MLP (FP32, ReLU) predicts, for every middle vertex of
  * the triangle kernel, log2 of the cycles each intersection variant (hash,
- * search, merge, bitmap: index 0..3) would take.  GARY_SCHED_LEARNED runs
+ * search, regs (at most 8 ids in registers), bitmap: index 0..3) would take.  GARY_SCHED_LEARNED runs
  * every warp vertex with its predicted-cheapest legal variant and cuts tiles
  * by predicted cycles; the plain plan (bitmap when the id span fits, else
  * hash; probe-count tile weights) stays the fallback.  No reference
