@@ -203,8 +203,11 @@ __global__ void __launch_bounds__(kSoWarps * 32)
         const uint32_t ls = a_short ? la : lb, ll = a_short ? lb : la;
         int v = variant;
         if (v == GARY_ISECT_AUTO) {
+          // search once the longer list exceeds half of |S| log2 |L| (measured
+          // on 2^20 Zipf pairs at overlap 0.1: 239 M pairs/s with the cut at
+          // 4 |S| log2 |L|, 285 M at 1x, 301 M at 1/2, 290 M at 1/4)
           const uint32_t lg = 32 - __clz(ll);
-          v = (uint64_t)ll > 4ull * ls * lg ? GARY_ISECT_SEARCH : GARY_ISECT_MERGE;
+          v = 2ull * ll > (uint64_t)ls * lg ? GARY_ISECT_SEARCH : GARY_ISECT_MERGE;
         }
         if (v == GARY_ISECT_MERGE) c2 = pair_merge(S, ls, L, ll, out, lane);
         else if (v == GARY_ISECT_SEARCH) c2 = pair_search(S, ls, L, ll, mine, out, lane);

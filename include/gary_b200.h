@@ -263,7 +263,7 @@ int gary_graph_drop_plans(gary_graph *g);
 
 /* ---- batched set operations: the include/ops layer ---------------------
  * Lists are sorted ascending, values < UINT32_MAX. */
-#define GARY_ISECT_AUTO 0   /* SEARCH when the longer list is much longer, else MERGE */
+#define GARY_ISECT_AUTO 0   /* SEARCH when 2|L| > |S| log2 |L| (L the longer list), else MERGE */
 #define GARY_ISECT_MERGE 1  /* warp merge path over 32-wide windows (ballot / shuffle) */
 #define GARY_ISECT_SEARCH 2 /* two-phase search: 256 shared samples, then HBM */
 #define GARY_ISECT_BITMAP 3 /* shared bitmap of the longer list over 32K-value windows */
