@@ -211,3 +211,36 @@ def test_unique_edges_match_symmetric_csr():
         pu, pv = O.unique_pairs(*O.sym_csr(s, d, n))
         assert np.array_equal(us, pu) and np.array_equal(vs, pv)
         assert np.all(us < vs)
+
+
+def _brute_counts(n: int, edges: set) -> tuple[int, int, int]:
+    """Triangles, 4-cycles and 4-cliques of a small graph by looking at every
+    3- and 4-vertex subset: a 4-set carries one of its three 4-cycles for each
+    cyclic order whose four edges exist, and is a 4-clique when all six do."""
+    e = lambda a, b: (min(a, b), max(a, b)) in edges  # noqa: E731
+    tri = sum(e(a, b) and e(b, c) and e(a, c) for a, b, c in itertools.combinations(range(n), 3))
+    c4 = k4 = 0
+    for a, b, c, d in itertools.combinations(range(n), 4):
+        c4 += (e(a, b) and e(b, c) and e(c, d) and e(d, a)) + (e(a, b) and e(b, d) and e(d, c) and e(c, a)) \
+            + (e(a, c) and e(c, b) and e(b, d) and e(d, a))
+        k4 += all(e(x, y) for x, y in itertools.combinations((a, b, c, d), 2))
+    return tri, c4, k4
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_pattern_oracle_against_brute_force(seed):
+    """The oracle's triangle, 4-cycle and 4-clique counts equal a brute-force
+    enumeration on random small graphs of every density (the reference has no
+    4-vertex pattern implementation to pin them to)."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(8, 19))
+    p = [0.15, 0.35, 0.6, 0.9][seed % 4]
+    edges = {(a, b) for a, b in itertools.combinations(range(n), 2) if rng.random() < p}
+    if not edges:
+        edges = {(0, 1)}
+    src = np.array([a for a, _ in edges], np.uint32)
+    dst = np.array([b for _, b in edges], np.uint32)
+    ptr, idx = O.sym_csr(src, dst, n)
+    dptr, didx = O.orient(ptr, idx)
+    got = (O.tri_count(dptr, didx), O.c4_count(ptr, idx), O.k4_count(dptr, didx))
+    assert got == _brute_counts(n, edges)
